@@ -1,0 +1,415 @@
+// qpgf.cuh -- quasi-periodic Helmholtz Green's function of a 2-D lattice (z non-periodic), FP64.
+//
+// Device (and host) re-implementation of the reference's d3hm_qpgf_d2_v1 / _qG / _dqG
+// (qgf2_src/d3_qpgf_d2.c:10-176) with the same mathematics, method choice and adaptive stop
+// rules, so that results agree with the reference to round-off:
+//
+//   G(r) = sum_l e^{i k|| . R_l} e^{ik|r+R_l|} / (4 pi |r+R_l|),   R_l = l1 d1 + l2 d2
+//
+//  * lattice reduction of r into the cell around the origin and the Bloch phase
+//    e^{-i k|| . (l1 d1 + l2 d2)} (d3_qpgf_d2.c:409-438, 290-319);
+//  * method choice (d3_qpgf_d2.c:124-176): the pure spectral (Fourier-domain, "FD") sum when
+//    no order +-S_LIMIT away from the central one propagates and the slowest evanescent order
+//    has decayed below eps at |z|, else the Ewald split ("EW");
+//  * EW: split parameter eps_E = sqrt(|det d|/(4 pi) |d1+d2|/|d1-d2|), lowered per point when
+//    k^2 eps_E^2 - |r|^2/(4 eps_E^2) > EW_EXPM (d3_qpgf_d2.c:1683-1693); real-space sum with
+//    Re w(k eps_E + i R/(2 eps_E)) terms (:1714-1838) and spectral sum with w / erfc terms
+//    (:1840-2009);
+//  * FD: plane-wave sum over reciprocal-lattice orders (:745-886).
+// Stop rules follow the reference's d3hm_sf_comp_z / d3hm_sf_diff_z (:471-482).
+//
+// Two stop-rule sets are provided:
+//   QP_V1   -- exactly the rules of d3hm_qpgf_d2_v1 (used by the regular element rules);
+//   QP_BOTH -- a row or a sum stops only once the rules of BOTH d3hm_qpgf_d2_qG and
+//              d3hm_qpgf_d2_dqG are met.  The singular element integrals of the reference
+//              call those two functions separately at every point (q0_bil_coef.c:444,489);
+//              one QP_BOTH evaluation returns both values, each summed at least as far as
+//              the reference sums it.
+#pragma once
+
+#include "cplx.cuh"
+#include "faddeeva.cuh"
+
+#define QP_S_LIMIT 15
+#define QP_FD_LIMIT 100
+#define QP_EW_LIMIT 100
+#define QP_EW_EXPM 3.0
+#define QP_EFS 0.1
+#define QP_MEPS 1.0e-15
+#define QP_PI 3.14159265358979323846
+#define QP_INV_SQRTPI 5.6418958354775628695e-1
+
+#define QP_V1 0
+#define QP_BOTH 1
+
+// Lattice and incidence constants.  Built once per problem on the host (qp_lattice_init)
+// with the same expressions as the reference so that derived values agree bit-for-bit.
+struct QPLattice {
+  double k;              // wave number of the periodic (open) domain
+  double vkx, vky;       // in-plane Bloch wave vector
+  double d1x, d1y, d2x, d2y;
+  double detd, idd;      // det[d1 d2], 1/det
+  double ad22;           // |d2|^2
+  double g1x, g1y, g2x, g2y;  // reciprocal vectors 2 pi idd (d2y,-d2x), 2 pi idd (-d1y, d1x)
+  double g22, g12;       // |g2|^2, g1.g2
+  double veps0;          // lattice Ewald split parameter
+  double bN, bNp, bNm;   // method selection (d3_qpgf_d2.c:135-155)
+  int ew_only;           // 1 when bNp>0 || bNm>0 (always Ewald)
+  int nc1;               // round(k||.d1 / 2 pi)
+};
+
+struct QPVal {
+  cplx G;
+  cplx dG[3];
+};
+
+BEM_HD int qp_comp(cplx a, cplx b, double eps)  // d3hm_sf_comp_z
+{
+  return (2.0 * fabs(a.re - b.re) <= eps * (fabs(a.re) + fabs(b.re))) &&
+         (2.0 * fabs(a.im - b.im) <= eps * (fabs(a.im) + fabs(b.im)));
+}
+BEM_HD int qp_diff(cplx v, cplx s, double eps)  // d3hm_sf_diff_z: |v| negligible against |s|
+{
+  return (fabs(v.re) <= fabs(s.re) * QP_EFS * eps) && (fabs(v.im) <= fabs(s.im) * QP_EFS * eps);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Ewald real-space term (d3_qpgf_d2.c:1814-1838).  F and dF[3] (dF[2] still lacks the
+// factor -z/(4 pi) that the sum applies at the end).
+BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1, int l2, cplx& F, cplx* dF)
+{
+  double Rl0 = (double)l1 * L.d1x + (double)l2 * L.d2x;
+  double Rl1 = (double)l1 * L.d1y + (double)l2 * L.d2y;
+  double px = r[0] + Rl0, py = r[1] + Rl1;
+  double rl = sqrt(px * px + py * py + r[2] * r[2]);
+  double i_rl = 1.0 / rl;
+  double ke = L.k * veps;
+  double i_ve = 1.0 / veps;
+  double rl_2e = rl * 0.5 * i_ve;
+  cplx ce = expi(L.vkx * Rl0 + L.vky * Rl1);
+  double ef = exp(ke * ke - rl_2e * rl_2e);
+  cplx w = faddeeva_w(ke, rl_2e);
+  double cfr = i_rl * i_rl * ef * (i_rl * w.re - L.k * w.im + i_ve * QP_INV_SQRTPI);
+  cplx cf = ce * cfr;
+  F = ce * (i_rl * ef * w.re);
+  dF[0] = px * cf;
+  dF[1] = py * cf;
+  dF[2] = cf;
+}
+
+// Ewald spectral term (d3_qpgf_d2.c:1965-2009).  Returns 0 propagating, 1 evanescent,
+// -3 when beta_n == 0 exactly.
+BEM_HD int qp_ew2_term(const QPLattice& L, const double* r, double veps, int n1, int n2, cplx& F, cplx* dF)
+{
+  double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
+  double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
+  double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
+  cplx ce = expi(an0 * r[0] + an1 * r[1]);
+  if (bn2 > 0.0) {
+    double bn = sqrt(bn2);
+    double azve = r[2] / (2.0 * veps);
+    double ef = exp(bn2 * veps * veps - azve * azve);
+    cplx ff = expi(bn * r[2]);
+    cplx w = faddeeva_w(bn * veps, azve);
+    // Fn = 2 ce / bn (i ef Im w + ff)
+    cplx t = mk(ff.re, ef * w.im + ff.im);
+    F = mk(2.0 * ce.re / bn, 2.0 * ce.im / bn) * t;
+    dF[0] = F * an0;
+    dF[1] = F * an1;
+    dF[2] = 2.0 * (ce * mk(ef * w.re - ff.re, -ff.im));
+    return 0;
+  } else if (bn2 < 0.0) {
+    double bn = sqrt(-bn2);
+    double azve = r[2] / (2.0 * veps);
+    double ebz = exp(bn * r[2]);
+    double f1 = ebz * erfc(bn * veps + azve);
+    double f2 = 1.0 / ebz * erfc(bn * veps - azve);
+    // Fn = ce / (i bn) (f1 + f2) = -i ce (f1+f2)/bn
+    F = mul_mi(ce * ((f1 + f2) / bn));
+    dF[0] = F * an0;
+    dF[1] = F * an1;
+    dF[2] = ce * (f1 - f2);
+    return 1;
+  }
+  return -3;
+}
+
+// Fourier-domain term (d3_qpgf_d2.c:856-885).  Returns 0 propagating, 1 evanescent, -2 if beta_n==0.
+BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx& F, cplx* dF)
+{
+  double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
+  double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
+  double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
+  if (bn2 > 0.0) {
+    double bn = sqrt(bn2);
+    dF[2] = expi(an0 * r[0] + an1 * r[1] + bn * fabs(r[2]));
+    F = dF[2] * (1.0 / bn);
+    dF[0] = F * an0;
+    dF[1] = F * an1;
+    return 0;
+  } else if (bn2 < 0.0) {
+    double bn = sqrt(-bn2);
+    dF[2] = expi(an0 * r[0] + an1 * r[1]) * exp(-bn * fabs(r[2]));
+    F = mul_mi(dF[2] * (1.0 / bn));
+    dF[0] = F * an0;
+    dF[1] = F * an1;
+    return 1;
+  }
+  return -2;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Ewald real-space sum (d3_qpgf_d2.c:1714-1812).  Returns the number of terms or -1.
+template <int MODE>
+BEM_HD int qp_ew1_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
+{
+  int cc = 0;
+  S = mk(0, 0); dS[0] = mk(0, 0); dS[1] = mk(0, 0); dS[2] = mk(0, 0);
+  cplx F, dF[3];
+  // l1 = 0, then l1 > 0, then l1 < 0
+  for (int dir = 0; dir < 3; dir++) {
+    int l1start = (dir == 0) ? 0 : (dir == 1 ? 1 : -1);
+    int step = (dir == 2) ? -1 : 1;
+    int l1;
+    for (l1 = l1start; (dir == 0) ? (l1 == 0) : (l1 * step < QP_EW_LIMIT); l1 += step) {
+      cplx oS = S, od0 = dS[0], od1 = dS[1];
+      // one row over l2 (d3_qpgf_d2.c:1762-1812)
+      int lc = -(int)round(((r[0] + (double)l1 * L.d1x) * L.d2x + (r[1] + (double)l1 * L.d1y) * L.d2y) / L.ad22);
+      qp_ew1_term(L, r, veps, l1, lc, F, dF);
+      S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
+      cc++;
+      for (int side = 0; side < 2; side++) {
+        int s2 = side ? -1 : 1;
+        int l2;
+        for (l2 = lc + s2; (l2 - lc) * s2 < QP_EW_LIMIT; l2 += s2) {
+          qp_ew1_term(L, r, veps, l1, l2, F, dF);
+          S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
+          cc++;
+          bool stop = qp_diff(F, S, eps);
+          if (MODE == QP_BOTH) stop = stop && qp_diff(dF[0], dS[0], eps) && qp_diff(dF[1], dS[1], eps);
+          if (stop) break;
+        }
+        if ((l2 - lc) * s2 >= QP_EW_LIMIT) return -1;
+      }
+      if (dir == 0) break;
+      bool stop = qp_comp(S, oS, eps);
+      if (MODE == QP_BOTH) stop = stop && qp_comp(dS[0], od0, eps) && qp_comp(dS[1], od1, eps);
+      if (stop) break;
+    }
+    if (dir != 0 && l1 * step >= QP_EW_LIMIT) return -1;
+  }
+  const double f4p = 4.0 * QP_PI;
+  S = mk(S.re / f4p, S.im / f4p);
+  dS[0] = mk(dS[0].re / -f4p, dS[0].im / -f4p);
+  dS[1] = mk(dS[1].re / -f4p, dS[1].im / -f4p);
+  dS[2] = dS[2] * (-r[2] / f4p);
+  return cc;
+}
+
+// Ewald spectral sum (d3_qpgf_d2.c:1840-1963).  Returns the number of terms or -2 / -3.
+template <int MODE>
+BEM_HD int qp_ew2_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
+{
+  int cc = 0;
+  S = mk(0, 0); dS[0] = mk(0, 0); dS[1] = mk(0, 0); dS[2] = mk(0, 0);
+  cplx F, dF[3];
+  const int nc = L.nc1;
+  for (int dir = 0; dir < 3; dir++) {
+    int n1start = (dir == 0) ? nc : (dir == 1 ? nc + 1 : nc - 1);
+    int step = (dir == 2) ? -1 : 1;
+    int n1;
+    for (n1 = n1start; (dir == 0) ? (n1 == nc) : ((n1 - nc) * step < QP_EW_LIMIT); n1 += step) {
+      cplx oS = S, od2 = dS[2];
+      // one row over n2 (d3_qpgf_d2.c:1902-1963)
+      int nc2 = (int)round(-((-L.vkx + (double)n1 * L.g1x) * L.g2x + (-L.vky + (double)n1 * L.g1y) * L.g2y) / L.g22);
+      int flg = 0;
+      int e = qp_ew2_term(L, r, veps, n1, nc2, F, dF);
+      cc++;
+      if (e < 0) return e;
+      S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
+      for (int side = 0; side < 2; side++) {
+        int s2 = side ? -1 : 1;
+        int n2;
+        for (n2 = nc2 + s2; (n2 - nc2) * s2 < QP_EW_LIMIT; n2 += s2) {
+          e = qp_ew2_term(L, r, veps, n1, n2, F, dF);
+          cc++;
+          if (e < 0) return e;
+          S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
+          if (e > 0) {
+            bool stop = qp_diff(dF[2], dS[2], eps);
+            if (MODE == QP_BOTH) stop = stop && qp_diff(F, S, eps);
+            if (stop) break;
+          } else {
+            flg++;
+          }
+        }
+        if ((n2 - nc2) * s2 >= QP_EW_LIMIT) return -2;
+      }
+      if (dir == 0) break;
+      if (flg == 0) {
+        bool stop = qp_comp(dS[2], od2, eps);
+        if (MODE == QP_BOTH) stop = stop && qp_comp(S, oS, eps);
+        if (stop) break;
+      }
+    }
+    if (dir != 0 && (n1 - nc) * step >= QP_EW_LIMIT) return -2;
+  }
+  const double aidd = fabs(L.idd);
+  S = mul_i(S * (0.25 * aidd));
+  dS[0] = dS[0] * (-0.25 * aidd);
+  dS[1] = dS[1] * (-0.25 * aidd);
+  dS[2] = dS[2] * (0.25 * aidd);
+  return cc;
+}
+
+// Fourier-domain sum (d3_qpgf_d2.c:745-854).  Returns the number of terms or -1/-2/-4.
+template <int MODE>
+BEM_HD int qp_fd_sum(const QPLattice& L, const double* r, double eps, cplx& S, cplx* dS)
+{
+  if (r[2] == 0.0) return -4;
+  int cc = 0;
+  S = mk(0, 0); dS[0] = mk(0, 0); dS[1] = mk(0, 0); dS[2] = mk(0, 0);
+  cplx F, dF[3];
+  const int nc = L.nc1;
+  for (int dir = 0; dir < 3; dir++) {
+    int n1start = (dir == 0) ? nc : (dir == 1 ? nc + 1 : nc - 1);
+    int step = (dir == 2) ? -1 : 1;
+    int n1;
+    for (n1 = n1start; (dir == 0) ? (n1 == nc) : ((n1 - nc) * step < QP_FD_LIMIT); n1 += step) {
+      cplx oS = S, od2 = dS[2];
+      int nc2 = (int)round((L.vkx * L.g2x + L.vky * L.g2y - (double)n1 * L.g12) / L.g22);
+      int e = qp_fd_term(L, r, n1, nc2, F, dF);
+      if (e < 0) return e;
+      S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
+      cc++;
+      for (int side = 0; side < 2; side++) {
+        int s2 = side ? -1 : 1;
+        int n2;
+        for (n2 = nc2 + s2; (n2 - nc2) * s2 < QP_FD_LIMIT; n2 += s2) {
+          e = qp_fd_term(L, r, n1, n2, F, dF);
+          if (e < 0) return e;
+          S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
+          cc++;
+          if (e > 0) {
+            bool stop = qp_diff(dF[2], dS[2], eps);
+            if (MODE == QP_BOTH) stop = stop && qp_diff(F, S, eps);
+            if (stop) break;
+          }
+        }
+        if ((n2 - nc2) * s2 >= QP_FD_LIMIT) return -1;
+      }
+      if (dir == 0) break;
+      bool stop = qp_comp(dS[2], od2, eps);
+      if (MODE == QP_BOTH) stop = stop && qp_comp(S, oS, eps);
+      if (stop) break;
+    }
+    if (dir != 0 && (n1 - nc) * step >= QP_FD_LIMIT) return -1;
+  }
+  const double aidd = fabs(L.idd);
+  S = mul_i(S * (0.5 * aidd));
+  dS[0] = dS[0] * (-0.5 * aidd);
+  dS[1] = dS[1] * (-0.5 * aidd);
+  dS[2] = dS[2] * (-0.5 * aidd * r[2] / fabs(r[2]));
+  return cc;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Full evaluation at r = (x, y, z): G and grad G.  Return value as the reference's
+// d3hm_qpgf_d2_v1: > 0 number of terms; -11..-14 FD errors; -21..-24 EW errors.
+template <int MODE>
+BEM_HD int qpgf_eval(const QPLattice& L, const double* r_in, QPVal& out)
+{
+  const double eps = QP_MEPS;
+  // lattice reduction (d3_qpgf_d2.c:417-423)
+  int l1 = (int)floor((r_in[0] * L.d2y - r_in[1] * L.d2x) * L.idd + 0.5);
+  int l2 = (int)floor(-(r_in[0] * L.d1y - r_in[1] * L.d1x) * L.idd + 0.5);
+  double r[3];
+  r[0] = r_in[0] - (double)l1 * L.d1x - (double)l2 * L.d2x;
+  r[1] = r_in[1] - (double)l1 * L.d1y - (double)l2 * L.d2y;
+  r[2] = r_in[2];
+
+  bool use_fd = false;
+  if (!L.ew_only) {
+    use_fd = (L.bN / L.bNp * exp(-L.bNp * fabs(r[2])) < eps) && (L.bN / L.bNm * exp(-L.bNm * fabs(r[2])) < eps);
+  }
+  int err;
+  if (use_fd) {
+    err = qp_fd_sum<MODE>(L, r, eps, out.G, out.dG);
+    if (err < 0) return err - 10;
+  } else {
+    // split parameter (d3_qpgf_d2.c:1683-1693)
+    double veps = L.veps0;
+    double r2_min = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    if (L.k * L.k * veps * veps - r2_min / (4.0 * veps * veps) > QP_EW_EXPM)
+      veps = sqrt(QP_EW_EXPM + sqrt(L.k * L.k * r2_min + QP_EW_EXPM * QP_EW_EXPM)) / (sqrt(2.0) * L.k);
+    cplx S2, dS2[3];
+    int c1 = qp_ew1_sum<MODE>(L, r, veps, eps, out.G, out.dG);
+    if (c1 < 0) return c1 - 20;
+    int c2 = qp_ew2_sum<MODE>(L, r, veps, eps, S2, dS2);
+    if (c2 < 0) return c2 - 20;
+    out.G += S2; out.dG[0] += dS2[0]; out.dG[1] += dS2[1]; out.dG[2] += dS2[2];
+    err = c1 + c2;
+  }
+  if (l1 != 0 || l2 != 0) {
+    double arg = -(L.vkx * ((double)l1 * L.d1x + (double)l2 * L.d2x) + L.vky * ((double)l1 * L.d1y + (double)l2 * L.d2y));
+    cplx cf = expi(arg);
+    out.G = out.G * cf;
+    out.dG[0] = out.dG[0] * cf;
+    out.dG[1] = out.dG[1] * cf;
+    out.dG[2] = out.dG[2] * cf;
+  }
+  return err;
+}
+
+// Lattice constants, following d3_qpgf_d2.c:129-155 (selection), :1680-1685 (split parameter)
+// and :1848-1857 (reciprocal vectors) expression by expression.
+BEM_HD int qp_lattice_init(QPLattice& L, double k, double vkx, double vky, double d1x, double d1y, double d2x, double d2y)
+{
+  L.k = k; L.vkx = vkx; L.vky = vky;
+  L.d1x = d1x; L.d1y = d1y; L.d2x = d2x; L.d2y = d2y;
+  L.detd = d1x * d2y - d2x * d1y;
+  if (L.detd == 0.0) return -1;
+  L.idd = 1.0 / L.detd;
+  double ad12 = d1x * d1x + d1y * d1y;
+  L.ad22 = d2x * d2x + d2y * d2y;
+  L.g1x = 2.0 * QP_PI * L.idd * d2y;
+  L.g1y = -2.0 * QP_PI * L.idd * d2x;
+  L.g2x = -2.0 * QP_PI * L.idd * d1y;
+  L.g2y = 2.0 * QP_PI * L.idd * d1x;
+  L.g22 = L.g2x * L.g2x + L.g2y * L.g2y;
+  L.g12 = L.g1x * L.g2x + L.g1y * L.g2y;
+  double adp = sqrt(pow(d1x + d2x, 2) + pow(d1y + d2y, 2));
+  double adm = sqrt(pow(d1x - d2x, 2) + pow(d1y - d2y, 2));
+  L.veps0 = sqrt(fabs(L.detd) / (4.0 * QP_PI) * adp / adm);
+  // method selection constants
+  double k2 = k * k, cpd = 2.0 * QP_PI * L.idd;
+  int n1 = (int)round((vkx * d1x + vky * d1y) / (2.0 * QP_PI));
+  int n2 = (int)round((vkx * d2x + vky * d2y) / (2.0 * QP_PI));
+  double aNx = -vkx + (double)n1 * cpd * d2y - (double)n2 * cpd * d1y;
+  double aNy = -vky - (double)n1 * cpd * d2x + (double)n2 * cpd * d1x;
+  L.bN = sqrt(k2 - aNx * aNx - aNy * aNy);
+  double aNpx, aNpy, aNmx, aNmy;
+  if (L.ad22 < ad12) {
+    aNpx = -vkx + (double)(n1 + QP_S_LIMIT) * cpd * d2y - (double)n2 * cpd * d1y;
+    aNpy = -vky - (double)(n1 + QP_S_LIMIT) * cpd * d2x + (double)n2 * cpd * d1x;
+    aNmx = -vkx + (double)(n1 - QP_S_LIMIT) * cpd * d2y - (double)n2 * cpd * d1y;
+    aNmy = -vky - (double)(n1 - QP_S_LIMIT) * cpd * d2x + (double)n2 * cpd * d1x;
+  } else {
+    aNpx = -vkx + (double)n1 * cpd * d2y - (double)(n2 + QP_S_LIMIT) * cpd * d1y;
+    aNpy = -vky - (double)n1 * cpd * d2x + (double)(n2 + QP_S_LIMIT) * cpd * d1x;
+    aNmx = -vkx + (double)n1 * cpd * d2y - (double)(n2 - QP_S_LIMIT) * cpd * d1y;
+    aNmy = -vky - (double)n1 * cpd * d2x + (double)(n2 - QP_S_LIMIT) * cpd * d1x;
+  }
+  double bNp = k2 - aNpx * aNpx - aNpy * aNpy;
+  double bNm = k2 - aNmx * aNmx - aNmy * aNmy;
+  if (bNp > 0.0 || bNm > 0.0) {
+    L.ew_only = 1;
+    L.bNp = 0.0; L.bNm = 0.0;
+  } else {
+    L.ew_only = 0;
+    L.bNp = sqrt(-bNp);
+    L.bNm = sqrt(-bNm);
+  }
+  L.nc1 = n1;
+  return 0;
+}
