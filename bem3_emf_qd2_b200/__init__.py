@@ -1,0 +1,209 @@
+"""bem3_emf_qd2_b200 -- B200 (sm_100a, FP64) boundary-integral hot path of bem3_emf_qd2.
+
+The compute runs in the CUDA library ``_lib/libbem3qd2.so`` (sources in ``csrc/``, C ABI in
+``include/bem3_qd2_b200.h``).  This module loads it with ctypes and offers numpy-level calls
+that mirror the reference's operator interface for the path:
+
+* ``qpgf(qd, r)``                       -- d3hm_qpgf_d2_v1 over many points (qgf2_src/d3_qpgf_d2.c:124)
+* ``assemble_domain(problem, did)``      -- create_cmatrix_domain (d3qd2_src/d3qd2_solve_bieq.c:165)
+
+There is no CPU fallback: if the library is missing or no CUDA device is present the calls
+raise ``RuntimeError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from .dqd2 import Problem  # noqa: F401  (re-exported)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libbem3qd2.so")
+REPO = os.path.dirname(HERE)
+
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+              "-diag-suppress", "20091", "-Xcompiler", "-fPIC", "-shared"]
+
+ERRORS = {
+    -1: "invalid argument", -2: "CUDA failure", -3: "scratch too small", -4: "degenerate lattice",
+    -5: "singular system", -900: "near-singular work list overflow",
+}
+
+
+def build(verbose: bool = False) -> str:
+    """Compile the CUDA library in-tree for sm_100a (nvcc cross-compiles without a GPU)."""
+    os.makedirs(os.path.dirname(LIB_PATH), exist_ok=True)
+    src = os.path.join(HERE, "csrc", "bem3_lib.cu")
+    cmd = ["nvcc", *NVCC_FLAGS, "-I" + os.path.join(REPO, "include"), "-I" + os.path.join(HERE, "csrc"),
+           src, "-o", LIB_PATH, "-lcusolver", "-lcublas"]
+    out = subprocess.run(cmd, capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + out.stdout[-6000:] + out.stderr[-6000:])
+    if verbose:
+        print(out.stdout + out.stderr)
+    return LIB_PATH
+
+
+class bem3_qpd2(C.Structure):
+    _fields_ = [("k", C.c_double), ("vk", C.c_double * 3), ("vd1", C.c_double * 2), ("vd2", C.c_double * 2)]
+
+
+class bem3_stats(C.Structure):
+    _fields_ = [("gh_pairs", C.c_ulonglong), ("qpgf_terms", C.c_ulonglong), ("launches", C.c_int),
+                ("reg_periodic_launches", C.c_int), ("reg_periodic_ms", C.c_double)]
+
+
+class bem3_mesh(C.Structure):
+    _fields_ = [("Ne", C.c_int), ("cr", C.c_void_p), ("cw", C.c_void_p), ("ren", C.c_void_p),
+                ("wen", C.c_void_p), ("nv", C.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"CUDA library not built: {LIB_PATH} (run bem3_emf_qd2_b200.build())")
+        L = C.CDLL(LIB_PATH)
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        L.bem3_qpgf.argtypes = [C.POINTER(bem3_qpd2), i, vp, vp, vp, i]
+        L.bem3_qpgf_dev.argtypes = [C.POINTER(bem3_qpd2), i, vp, vp, vp, i, vp]
+        L.bem3_assemble_domain.argtypes = [C.POINTER(bem3_mesh), vp, i, i, i, C.POINTER(bem3_qpd2), d, d,
+                                           vp, vp, vp, vp, vp]
+        L.bem3_assemble_domain_dev.argtypes = [vp, i, vp, i, i, i, C.POINTER(bem3_qpd2), d, d, vp, vp, vp, vp, vp, vp]
+        L.bem3_pack_geometry.argtypes = [C.POINTER(bem3_mesh), vp]
+        L.bem3_geo_stride.restype = i
+        L.bem3_last_gh_pairs.restype = C.c_ulonglong
+        L.bem3_gauss_legendre.argtypes = [i, vp, vp]
+        L.bem3_version.restype = C.c_char_p
+        L.bem3_set_profiling.argtypes = [i]
+        L.bem3_last_stats.argtypes = [C.POINTER(bem3_stats)]
+        L.bem3_fp64_peak_tflops.restype = d
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise RuntimeError(f"{what} failed: {rc} ({ERRORS.get(rc, 'quasi-periodic Green function failure')})")
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def make_qpd(qpd: dict) -> bem3_qpd2:
+    q = bem3_qpd2()
+    q.k = qpd["k"]
+    for j in range(3):
+        q.vk[j] = qpd["vk"][j]
+    for j in range(2):
+        q.vd1[j] = qpd["vd1"][j]
+        q.vd2[j] = qpd["vd2"][j]
+    return q
+
+
+def qpgf(qpd: dict, r: np.ndarray, mode: int = 0):
+    """Green's function and gradient at points r[n,3].  Returns (out[n,4] complex, ret[n])."""
+    r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+    n = len(r)
+    out = np.zeros((n, 4), np.complex128)
+    ret = np.zeros(n, np.int32)
+    q = make_qpd(qpd)
+    check(lib().bem3_qpgf(C.byref(q), n, _ptr(r), _ptr(out), _ptr(ret), mode), "bem3_qpgf")
+    return out, ret
+
+
+class MeshArrays:
+    """Keeps the flattened mesh arrays alive while a bem3_mesh points at them."""
+
+    def __init__(self, problem: Problem):
+        self.cr, self.cw, self.ren, self.wen, self.nv = problem.flat_mesh()
+        self.m = bem3_mesh(problem.Ne, _ptr(self.cr), _ptr(self.cw), _ptr(self.ren), _ptr(self.wen), _ptr(self.nv))
+
+    def packed(self) -> np.ndarray:
+        stride = lib().bem3_geo_stride()
+        geo = np.zeros((self.m.Ne + 1) * stride)
+        check(lib().bem3_pack_geometry(C.byref(self.m), _ptr(geo)), "bem3_pack_geometry")
+        return geo
+
+
+def assemble_domain(problem: Problem, did: int, derivatives: bool = True):
+    """Coefficient matrices of domain `did` on the GPU (host in, host out).
+
+    Returns dict G, H [N,N], dG, dH [2N,N] (complex), dF [N,3] with N = 4 Ne_d, in the layout of
+    the reference's temp files (d3qd2_solve_bieq.c:213-236)."""
+    sid = np.ascontiguousarray(problem.sid[did], dtype=np.int32)
+    ne = len(sid)
+    N = 4 * ne
+    G = np.zeros((N, N), np.complex128)
+    H = np.zeros((N, N), np.complex128)
+    dG = np.zeros((2 * N, N), np.complex128) if derivatives else None
+    dH = np.zeros((2 * N, N), np.complex128) if derivatives else None
+    dF = np.zeros((N, 3))
+    ma = MeshArrays(problem)
+    q = make_qpd(problem.qpd)
+    periodic = 1 if (did == 0 and problem.ps == 1) else 0
+    k = complex(problem.kn[did])
+    rc = lib().bem3_assemble_domain(C.byref(ma.m), _ptr(sid), ne, did, periodic, C.byref(q), k.real, k.imag,
+                                    _ptr(G), _ptr(H), _ptr(dG) if dG is not None else None,
+                                    _ptr(dH) if dH is not None else None, _ptr(dF))
+    check(rc, "bem3_assemble_domain")
+    return dict(G=G, H=H, dG=dG, dH=dH, dF=dF, gh_pairs=int(lib().bem3_last_gh_pairs()))
+
+
+def gauss_legendre(n: int):
+    x = np.zeros(n)
+    w = np.zeros(n)
+    lib().bem3_gauss_legendre(n, _ptr(x), _ptr(w))
+    return x, w
+
+
+def last_stats() -> dict:
+    st = bem3_stats()
+    lib().bem3_last_stats(C.byref(st))
+    return {f: getattr(st, f) for f, _ in bem3_stats._fields_}
+
+
+def set_profiling(on: bool) -> None:
+    lib().bem3_set_profiling(1 if on else 0)
+
+
+def fp64_peak_tflops() -> float:
+    return float(lib().bem3_fp64_peak_tflops())
+
+
+class DeviceProblem:
+    """Geometry resident in HBM plus output buffers sized for the largest domain (torch tensors
+    used as device allocations only).  ``assemble(did, stream)`` runs one domain through
+    bem3_assemble_domain_dev."""
+
+    def __init__(self, problem: Problem, device="cuda"):
+        import torch
+        self.p = problem
+        ma = MeshArrays(problem)
+        self.geo = torch.from_numpy(ma.packed()).to(device)
+        self.sids = [torch.from_numpy(np.ascontiguousarray(s, dtype=np.int32)).to(device) for s in problem.sid]
+        nmax = max(4 * len(s) for s in problem.sid)
+        self.G = torch.empty((nmax, nmax), dtype=torch.complex128, device=device)
+        self.H = torch.empty_like(self.G)
+        self.dG = torch.empty((2 * nmax, nmax), dtype=torch.complex128, device=device)
+        self.dH = torch.empty_like(self.dG)
+        self.dF = torch.empty((nmax, 3), dtype=torch.float64, device=device)
+        self.q = make_qpd(problem.qpd)
+
+    def assemble(self, did: int, stream=None) -> None:
+        k = complex(self.p.kn[did])
+        ne = len(self.p.sid[did])
+        periodic = 1 if (did == 0 and self.p.ps == 1) else 0
+        rc = lib().bem3_assemble_domain_dev(self.geo.data_ptr(), self.p.Ne, self.sids[did].data_ptr(), ne, did,
+                                            periodic, C.byref(self.q), k.real, k.imag, self.G.data_ptr(),
+                                            self.H.data_ptr(), self.dG.data_ptr(), self.dH.data_ptr(),
+                                            self.dF.data_ptr(), stream)
+        check(rc, "bem3_assemble_domain_dev")

@@ -1,0 +1,580 @@
+// assemble.cu -- sm_100a kernels for the coefficient-matrix assembly of one domain
+// (the reference's create_cmatrix_domain, d3qd2_src/d3qd2_solve_bieq.c:165-256).
+//
+// Output layout is the reference's (d3qd2_solve_bieq.c:213-236), N = 4 * Ne_d:
+//   G, H   [N][N]     row (t,tn) = 4 t + tn, column (s,i) = 4 s + i        (complex)
+//   dG, dH [2N][N]    row 2 (4 t + tn) + {0: d/dt_zeta, 1: d/dt_eta}       (complex)
+//   dF     [N][3]     (F or 1+F, dF/dt_zeta, dF/dt_eta)                   (double)
+// with 0-based t, s indexing sb[did].sid.  Rows tn = 3 of triangles are left zero, as in
+// the reference.
+//
+// Work decomposition (all FP64, no tensor cores -- none of this is a contraction):
+//   k_self_periodic / k_self_interior : one CTA per self pair (t == s), polar rule;
+//   k_reg_periodic : one warp per regular pair, lanes over the 144 (quad) / 432 (triangle)
+//                    Gauss points, one quasi-periodic Green's function per point;
+//   k_reg_interior : one thread per regular pair (free-space kernel, uniform cost);
+//   k_gh_*         : pairs whose GL dF/dv exceeds CBD_SDF, recomputed with the 64x64 rule from a
+//                    compacted device work list (no host round trip);
+//   k_rowsum       : deterministic per-row sums of F, dF/dt over s, H diagonal += (1+)F.
+// Regular pairs run in row chunks so that the per-pair F scratch stays bounded.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <vector>
+
+#include "elem.cuh"
+#include "bem3_internal.h"
+
+// ------------------------------------------------------------------------------------------
+// Constant tables: Gauss-Legendre nodes (12, 64) and the open-domain lattice.
+__constant__ double c_xl[12], c_wl[12], c_xh[64], c_wh[64];
+
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_min_i(int v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+template <int N>
+__device__ __forceinline__ void warp_sum_arr(double* v)
+{
+#pragma unroll
+  for (int i = 0; i < N; i++) v[i] = warp_sum(v[i]);
+}
+
+__device__ __forceinline__ void record_status(int* status, int err)
+{
+  if (err < 0) atomicCAS(status, 0, err);
+}
+
+struct PairIdx {
+  int row, s, t, tn;
+};
+__device__ __forceinline__ PairIdx pair_of(long long p, int ne)
+{
+  PairIdx q;
+  q.row = (int)(p / ne);
+  q.s = (int)(p - (long long)q.row * ne);
+  q.t = q.row >> 2;
+  q.tn = q.row & 3;
+  return q;
+}
+
+__device__ __forceinline__ void target_info(const double* __restrict__ geo, const int* __restrict__ sid, int t, int tn,
+                                            double* rt, double* vtz, double* vte, int& tnn)
+{
+  int at = abs(sid[t]);
+  Elem et;
+  load_elem(geo, at, et);
+  tnn = et.nn;
+  node_tangents(et, tn, vtz, vte);
+  const double* g = geo + (size_t)at * GEO_STRIDE + GEO_REN + tn * 3;
+  rt[0] = g[0]; rt[1] = g[1]; rt[2] = g[2];
+}
+
+// AccP <-> flat array (19 doubles)
+__device__ __forceinline__ void accp_pack(const AccP& a, double* v)
+{
+  for (int i = 0; i < 4; i++) { v[2 * i] = a.G[i].re; v[2 * i + 1] = a.G[i].im; v[8 + 2 * i] = a.H[i].re; v[9 + 2 * i] = a.H[i].im; }
+  v[16] = a.F; v[17] = a.dF0; v[18] = a.dF1;
+}
+__device__ __forceinline__ void accp_unpack(const double* v, AccP& a)
+{
+  for (int i = 0; i < 4; i++) { a.G[i] = mk(v[2 * i], v[2 * i + 1]); a.H[i] = mk(v[8 + 2 * i], v[9 + 2 * i]); }
+  a.F = v[16]; a.dF0 = v[17]; a.dF1 = v[18];
+}
+// AccI <-> flat array (51 doubles)
+__device__ __forceinline__ void acci_pack(const AccI& a, double* v)
+{
+  for (int i = 0; i < 4; i++) {
+    v[2 * i] = a.G[i].re; v[2 * i + 1] = a.G[i].im;
+    v[8 + 2 * i] = a.H[i].re; v[9 + 2 * i] = a.H[i].im;
+    v[16 + 2 * i] = a.dG0[i].re; v[17 + 2 * i] = a.dG0[i].im;
+    v[24 + 2 * i] = a.dH0[i].re; v[25 + 2 * i] = a.dH0[i].im;
+    v[32 + 2 * i] = a.dG1[i].re; v[33 + 2 * i] = a.dG1[i].im;
+    v[40 + 2 * i] = a.dH1[i].re; v[41 + 2 * i] = a.dH1[i].im;
+  }
+  v[48] = a.F; v[49] = a.dF0; v[50] = a.dF1;
+}
+__device__ __forceinline__ void acci_unpack(const double* v, AccI& a)
+{
+  for (int i = 0; i < 4; i++) {
+    a.G[i] = mk(v[2 * i], v[2 * i + 1]); a.H[i] = mk(v[8 + 2 * i], v[9 + 2 * i]);
+    a.dG0[i] = mk(v[16 + 2 * i], v[17 + 2 * i]); a.dH0[i] = mk(v[24 + 2 * i], v[25 + 2 * i]);
+    a.dG1[i] = mk(v[32 + 2 * i], v[33 + 2 * i]); a.dH1[i] = mk(v[40 + 2 * i], v[41 + 2 * i]);
+  }
+  a.F = v[48]; a.dF0 = v[49]; a.dF1 = v[50];
+}
+
+// Store one pair's coefficients in the reference layout.  Done by lanes of a warp (lane l
+// stores item l) or by a single thread (lane = -1 stores all).
+__device__ __forceinline__ void store_pair(const AssembleArgs& A, int row, int s, const cplx* CC, const cplx* dCz,
+                                           const cplx* dCe, double3* Fp, long long fidx, int lane)
+{
+  const size_t N = (size_t)4 * A.ne;
+  const size_t col = (size_t)4 * s;
+  cplx* G = (cplx*)A.G;
+  cplx* H = (cplx*)A.H;
+  cplx* dG = (cplx*)A.dG;
+  cplx* dH = (cplx*)A.dH;
+  for (int it = (lane < 0 ? 0 : lane); it < 25; it += (lane < 0 ? 1 : 32)) {
+    if (it < 4) G[(size_t)row * N + col + it] = CC[it];
+    else if (it < 8) H[(size_t)row * N + col + it - 4] = CC[it];
+    else if (it < 12) { if (dG) dG[(size_t)(2 * row) * N + col + it - 8] = dCz[it - 8]; }
+    else if (it < 16) { if (dG) dG[(size_t)(2 * row + 1) * N + col + it - 12] = dCe[it - 12]; }
+    else if (it < 20) { if (dH) dH[(size_t)(2 * row) * N + col + it - 16] = dCz[it - 12]; }
+    else if (it < 24) { if (dH) dH[(size_t)(2 * row + 1) * N + col + it - 20] = dCe[it - 16]; }
+    else Fp[fidx] = make_double3(CC[8].re, dCz[8].re, dCe[8].re);
+  }
+}
+
+// ==========================================================================================
+// Regular periodic pairs: one warp per pair.
+__global__ void __launch_bounds__(256, 1) k_reg_periodic(AssembleArgs A, QPLattice L, long long p0, long long np,
+                                                      double3* Fp, unsigned* gh_list, unsigned* gh_count,
+                                                      unsigned gh_cap, int* status)
+{
+  long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (w >= np) return;
+  long long p = p0 + w;
+  PairIdx q = pair_of(p, A.ne);
+  int tnn;
+  double rt[3], vtz[3], vte[3];
+  target_info(A.geo, A.sid, q.t, q.tn, rt, vtz, vte, tnn);
+  if ((q.tn == 3 && tnn == 3) || q.s == q.t) return;
+  Elem es;
+  load_elem(A.geo, abs(A.sid[q.s]), es);
+  const int npts = (es.nn == 4) ? 144 : 432;
+  AccP a;
+  accp_zero(a);
+  int err = 0, nterms = 0;
+  for (int k = lane; k < npts; k += 32) {
+    double z, e, wt;
+    rule_point(es.nn, 12, c_xl, c_wl, k, z, e, wt);
+    int e2 = accp_point(es, L, rt, vtz, vte, z, e, wt, a);
+    if (e2 < 0) err = e2;
+    else nterms += e2;
+  }
+  double v[19];
+  accp_pack(a, v);
+  warp_sum_arr<19>(v);
+  accp_unpack(v, a);
+  err = warp_min_i(err);
+  if (lane == 0) record_status(status, err);
+  if (A.terms) {
+    double tc = warp_sum((double)nterms);
+    if (lane == 0) atomicAdd(A.terms, (unsigned long long)tc);
+  }
+  cplx CC[9], dCz[9], dCe[9];
+  accp_finish(es, a, CC, dCz, dCe);
+  if (needs_gh(dCz[8].re, dCe[8].re)) {
+    if (lane == 0) {
+      unsigned slot = atomicAdd(gh_count, 1u);
+      if (slot < gh_cap) gh_list[slot] = (unsigned)w;
+      else record_status(status, -900);
+    }
+    return;
+  }
+  store_pair(A, q.row, q.s, CC, dCz, dCe, Fp, w, lane);
+}
+
+// Near-singular periodic pairs: one CTA (256 threads) per listed pair, 64x64 rule.
+__global__ void __launch_bounds__(256, 1) k_gh_periodic(AssembleArgs A, QPLattice L, long long p0, double3* Fp,
+                                                     const unsigned* gh_list, const unsigned* gh_count, int* status)
+{
+  __shared__ double red[8][19];
+  __shared__ int serr[8];
+  unsigned n = *gh_count;
+  for (unsigned it = blockIdx.x; it < n; it += gridDim.x) {
+    long long w = gh_list[it];
+    PairIdx q = pair_of(p0 + w, A.ne);
+    int tnn;
+    double rt[3], vtz[3], vte[3];
+    target_info(A.geo, A.sid, q.t, q.tn, rt, vtz, vte, tnn);
+    Elem es;
+    load_elem(A.geo, abs(A.sid[q.s]), es);
+    AccP a;
+    accp_zero(a);
+    int err = 0;
+    const int npts = (es.nn == 4) ? 4096 : 3 * 4096;
+    for (int k = threadIdx.x; k < npts; k += blockDim.x) {
+      double z, e, wt;
+      rule_point(es.nn, 64, c_xh, c_wh, k, z, e, wt);
+      int e2 = accp_point(es, L, rt, vtz, vte, z, e, wt, a);
+      if (e2 < 0) err = e2;
+    }
+    double v[19];
+    accp_pack(a, v);
+    warp_sum_arr<19>(v);
+    err = warp_min_i(err);
+    int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { for (int i = 0; i < 19; i++) red[wid][i] = v[i]; serr[wid] = err; }
+    __syncthreads();
+    if (wid == 0) {
+      for (int i = 0; i < 19; i++) v[i] = (lane < 8) ? red[lane][i] : 0.0;
+      warp_sum_arr<19>(v);
+      int e3 = warp_min_i(lane < 8 ? serr[lane] : 0);
+      if (lane == 0) record_status(status, e3);
+      accp_unpack(v, a);
+      cplx CC[9], dCz[9], dCe[9];
+      accp_finish(es, a, CC, dCz, dCe);
+      store_pair(A, q.row, q.s, CC, dCz, dCe, Fp, w, lane);
+    }
+    __syncthreads();
+  }
+}
+
+// ==========================================================================================
+// Regular interior pairs: one thread per pair.
+__global__ void __launch_bounds__(128) k_reg_interior(AssembleArgs A, long long p0, long long np, double3* Fp,
+                                                      unsigned* gh_list, unsigned* gh_count, unsigned gh_cap, int* status)
+{
+  long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= np) return;
+  long long p = p0 + w;
+  PairIdx q = pair_of(p, A.ne);
+  int tnn;
+  double rt[3], vtz[3], vte[3];
+  target_info(A.geo, A.sid, q.t, q.tn, rt, vtz, vte, tnn);
+  if ((q.tn == 3 && tnn == 3) || q.s == q.t) return;
+  int sd = A.sid[q.s];
+  Elem es;
+  load_elem(A.geo, abs(sd), es);
+  const int npts = (es.nn == 4) ? 144 : 432;
+  const cplx k = mk(A.kre, A.kim);
+  AccI a;
+  acci_zero(a);
+  for (int kq = 0; kq < npts; kq++) {
+    double z, e, wt;
+    rule_point(es.nn, 12, c_xl, c_wl, kq, z, e, wt);
+    acci_point(es, k, rt, vtz, vte, z, e, wt, a);
+  }
+  cplx CC[9], dCz[9], dCe[9];
+  acci_finish(es, a, sd < 0, CC, dCz, dCe);
+  if (needs_gh(dCz[8].re, dCe[8].re)) {
+    unsigned slot = atomicAdd(gh_count, 1u);
+    if (slot < gh_cap) gh_list[slot] = (unsigned)w;
+    else record_status(status, -900);
+    return;
+  }
+  store_pair(A, q.row, q.s, CC, dCz, dCe, Fp, w, -1);
+}
+
+// Near-singular interior pairs: one warp per listed pair, 64x64 rule.
+__global__ void __launch_bounds__(256) k_gh_interior(AssembleArgs A, long long p0, double3* Fp, const unsigned* gh_list,
+                                                     const unsigned* gh_count)
+{
+  unsigned n = *gh_count;
+  int lane = threadIdx.x & 31;
+  unsigned wglob = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  unsigned nw = (gridDim.x * blockDim.x) >> 5;
+  const cplx k = mk(A.kre, A.kim);
+  for (unsigned it = wglob; it < n; it += nw) {
+    long long w = gh_list[it];
+    PairIdx q = pair_of(p0 + w, A.ne);
+    int tnn;
+    double rt[3], vtz[3], vte[3];
+    target_info(A.geo, A.sid, q.t, q.tn, rt, vtz, vte, tnn);
+    int sd = A.sid[q.s];
+    Elem es;
+    load_elem(A.geo, abs(sd), es);
+    const int npts = (es.nn == 4) ? 4096 : 3 * 4096;
+    AccI a;
+    acci_zero(a);
+    for (int kq = lane; kq < npts; kq += 32) {
+      double z, e, wt;
+      rule_point(es.nn, 64, c_xh, c_wh, kq, z, e, wt);
+      acci_point(es, k, rt, vtz, vte, z, e, wt, a);
+    }
+    double v[51];
+    acci_pack(a, v);
+    warp_sum_arr<51>(v);
+    acci_unpack(v, a);
+    cplx CC[9], dCz[9], dCe[9];
+    acci_finish(es, a, sd < 0, CC, dCz, dCe);
+    store_pair(A, q.row, q.s, CC, dCz, dCe, Fp, w, lane);
+  }
+}
+
+// ==========================================================================================
+// Row sums (d3qd2_solve_bieq.c:222-236): F, dF/dtz, dF/dte over all s (regular pairs from the
+// chunk scratch, the self pair from Fself), then H[row][4t+tn] += (did==0 ? 1 : 0) + F.
+// One warp per row; lane-strided partial sums and a fixed-shape reduction (deterministic).
+__global__ void k_rowsum(AssembleArgs A, int row0, int nrows, const double3* Fp, const double3* Fself)
+{
+  int wr = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (wr >= nrows) return;
+  int row = row0 + wr;
+  int t = row >> 2, tn = row & 3;
+  int at = abs(A.sid[t]);
+  int tnn = (int)A.geo[(size_t)at * GEO_STRIDE + GEO_NN];
+  if (tn == 3 && tnn == 3) return;
+  double f0 = 0, f1 = 0, f2 = 0;
+  const double3* fr = Fp + (size_t)wr * A.ne;
+  for (int s = lane; s < A.ne; s += 32) {
+    if (s == t) continue;
+    double3 v = fr[s];
+    f0 += v.x; f1 += v.y; f2 += v.z;
+  }
+  f0 = warp_sum(f0); f1 = warp_sum(f1); f2 = warp_sum(f2);
+  if (lane == 0) {
+    double3 sv = Fself[row];
+    f0 += sv.x; f1 += sv.y; f2 += sv.z;
+    double diag = (A.did == 0) ? 1.0 + f0 : f0;
+    cplx* H = (cplx*)A.H;
+    size_t N = (size_t)4 * A.ne;
+    H[(size_t)row * N + 4 * (size_t)t + tn].re += diag;
+    if (A.dF) {
+      A.dF[3 * (size_t)row + 0] = diag;
+      A.dF[3 * (size_t)row + 1] = f1;
+      A.dF[3 * (size_t)row + 2] = f2;
+    }
+  }
+}
+
+// ==========================================================================================
+// Self pairs of the periodic domain (q0_bil_dcoef_bd_vt2_cc_DV q0_bil_dcoef_v2_cc.c:292-301 and
+// q0_lit_dcoef_bd_vt2_cc_DV q0_lit_dcoef_v2_cc.c:331-342).  One CTA per (t, tn).
+#define SELF_THREADS 256
+__global__ void __launch_bounds__(SELF_THREADS, 1) k_self_periodic(AssembleArgs A, QPLattice L, double3* Fself, int* status)
+{
+  __shared__ double red[SELF_THREADS / 32][24];
+  __shared__ int serr[SELF_THREADS / 32];
+  const int row = blockIdx.x;
+  const int t = row >> 2, tn = row & 3;
+  const int sd = A.sid[t];
+  const int at = abs(sd);
+  Elem e;
+  load_elem(A.geo, at, e);
+  if (tn == 3 && e.nn == 3) return;
+  const double zt = node_zeta(e.nn, tn), et = node_eta(e.nn, tn);
+  PolarSet P;
+  polar_setup(e.nn, zt, et, P);
+  const int npts = P.nsub * 128 * 12;
+  cplx G[4], H[4];
+  for (int i = 0; i < 4; i++) { G[i] = mk(0, 0); H[i] = mk(0, 0); }
+  int err = 0;
+  for (int k = threadIdx.x; k < npts; k += blockDim.x) {
+    int ir = k % 12;
+    int tq = k / 12;
+    int j = tq >> 7, m2 = tq & 127;
+    double theta, wt;
+    polar_theta(P, j, m2, c_xh, c_wh, theta, wt);
+    double rm = polar_rm(P, j, theta);
+    double cth = cos(theta), sth = sin(theta);
+    double r = 0.5 * rm * (c_xl[ir] + 1.0);
+    double w = wt * 0.5 * rm * c_wl[ir];
+    double zeta = r * cth + zt, eta = r * sth + et;
+    double vR[3], W[3], N[4];
+    if (e.nn == 4) {
+      double K[3];
+      bil_K(e, zt, et, r, cth, sth, K);
+      for (int i = 0; i < 3; i++) {
+        vR[i] = r * K[i];
+        W[i] = e.cw[i][0] + e.cw[i][1] * zeta + e.cw[i][2] * eta;
+      }
+      bil_N4(zeta, eta, N);
+    } else {
+      for (int i = 0; i < 3; i++) {
+        vR[i] = r * (e.cr[i][1] * cth + e.cr[i][2] * sth);
+        W[i] = e.cw[i][0];
+      }
+      lit_N3(zeta, eta, N);
+      N[3] = 0.0;
+    }
+    QPVal g;
+    int e2 = qpgf_eval<QP_BOTH>(L, vR, g);
+    if (e2 < 0) err = e2;
+    double aW = (e.nn == 4) ? vnorm3(W) : 1.0;
+    cplx gw = g.G * (w * aW * r);
+    cplx hw = (g.dG[0] * W[0] + g.dG[1] * W[1] + g.dG[2] * W[2]) * (w * r);
+    for (int i = 0; i < 4; i++) { G[i] += gw * N[i]; H[i] += hw * N[i]; }
+  }
+  // curved quads: F at the node and at the four finite-difference neighbours
+  double Fv[5] = {0, 0, 0, 0, 0};
+  if (e.nn == 4 && !bil_is_plane(e)) {
+    const double h = EL_CDFH;
+    const double cz[5] = {zt, zt + h, zt - h, zt, zt};
+    const double ce[5] = {et, et, et, et + h, et - h};
+    for (int c = 0; c < 5; c++) Fv[c] = bil_self_F(e, cz[c], ce[c], c_xl, c_wl, c_xh, c_wh, threadIdx.x, blockDim.x);
+  }
+  double v[24];
+  for (int i = 0; i < 4; i++) { v[2 * i] = G[i].re; v[2 * i + 1] = G[i].im; v[8 + 2 * i] = H[i].re; v[9 + 2 * i] = H[i].im; }
+  for (int c = 0; c < 5; c++) v[16 + c] = Fv[c];
+  v[21] = v[22] = v[23] = 0.0;
+  warp_sum_arr<24>(v);
+  err = warp_min_i(err);
+  int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { for (int i = 0; i < 24; i++) red[wid][i] = v[i]; serr[wid] = err; }
+  __syncthreads();
+  if (wid != 0) return;
+  for (int i = 0; i < 24; i++) v[i] = (lane < SELF_THREADS / 32) ? red[lane][i] : 0.0;
+  warp_sum_arr<24>(v);
+  int e3 = warp_min_i(lane < SELF_THREADS / 32 ? serr[lane] : 0);
+  if (lane != 0) return;
+  record_status(status, e3);
+  cplx CC[9], dCz[9], dCe[9];
+  for (int i = 0; i < 9; i++) { CC[i] = mk(0, 0); dCz[i] = mk(0, 0); dCe[i] = mk(0, 0); }
+  if (e.nn == 4) {
+    for (int i = 0; i < 4; i++) { CC[i] = mk(v[2 * i], v[2 * i + 1]); CC[i + 4] = mk(v[8 + 2 * i], v[9 + 2 * i]); }
+    double bdC = e.cr[0][1] * e.cw[0][2] + e.cr[1][1] * e.cw[1][2] + e.cr[2][1] * e.cw[2][2];
+    double s = EL_I_FP * bdC;
+    CC[8] = mk(v[16] * s, 0);
+    // dF/dt by central differences (q0_bil_dcoef_bd_tz0_cc_DV :336-362, te0 :364-390)
+    double Tz[3], Te[3];
+    for (int i = 0; i < 3; i++) { Tz[i] = e.cr[i][1] + e.cr[i][3] * et; Te[i] = e.cr[i][2] + e.cr[i][3] * zt; }
+    dCz[8] = mk(1.0 / vnorm3(Tz) * (v[17] * s - v[18] * s) / (2.0 * EL_CDFH), 0);
+    dCe[8] = mk(1.0 / vnorm3(Te) * (v[19] * s - v[20] * s) / (2.0 * EL_CDFH), 0);
+  } else {
+    double V[3] = {e.cw[0][0], e.cw[1][0], e.cw[2][0]};
+    double aV = vnorm3(V);
+    for (int i = 0; i < 3; i++) {
+      CC[i] = mk(v[2 * i], v[2 * i + 1]) * (2.0 / (3.0 * EL_SQ3) * aV);
+      CC[i + 4] = mk(v[8 + 2 * i], v[9 + 2 * i]) * (2.0 / (3.0 * EL_SQ3));
+    }
+  }
+  store_pair(A, row, t, CC, dCz, dCe, Fself, row, -1);
+}
+
+// ==========================================================================================
+// Host side
+static void gauleg_host(int n, double* x, double* w)
+{
+  // Gauss-Legendre nodes on [-1,1] by Newton iteration on P_n from the Chebyshev-like initial
+  // guess, with the stop tolerance of the reference's gauleg (com_src/gauleg.c:3-36) so that the
+  // tables agree bit for bit (near-singular pairs are sensitive to the last bits of the nodes).
+  for (int i = 0; i < (n + 1) / 2; i++) {
+    double z = cos(QP_PI * (i + 0.75) / (n + 0.5)), z1, pp;
+    for (int it = 0; it < 100; it++) {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= n; j++) {
+        double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+      if (fabs(z - z1) <= 3.0e-16) break;
+    }
+    x[i] = -z;
+    x[n - 1 - i] = z;
+    w[i] = 2.0 / ((1.0 - z * z) * pp * pp);
+    w[n - 1 - i] = w[i];
+  }
+}
+
+static int g_tables_ready[64];
+
+static int ensure_tables(void)
+{
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && g_tables_ready[dev]) return 0;
+  double xl[12], wl[12], xh[64], wh[64];
+  gauleg_host(12, xl, wl);
+  gauleg_host(64, xh, wh);
+  if (cudaMemcpyToSymbol(c_xl, xl, sizeof xl) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(c_wl, wl, sizeof wl) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(c_xh, xh, sizeof xh) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(c_wh, wh, sizeof wh) != cudaSuccess) return -1;
+  if (dev < 64) g_tables_ready[dev] = 1;
+  return 0;
+}
+
+extern "C" void bem3_gauss_legendre(int n, double* x, double* w) { gauleg_host(n, x, w); }
+
+// Scratch needed for a chunk of `rows` rows: Fp (rows*ne double3) + GH list (rows*ne/8 + 4096 u32)
+size_t bem3_scratch_bytes(int ne, int rows)
+{
+  size_t np = (size_t)rows * ne;
+  size_t fp = np * sizeof(double3);
+  size_t gh = (np / 8 + 4096) * sizeof(unsigned);
+  return fp + gh + 256 + (size_t)4 * ne * sizeof(double3) + 256;
+}
+
+// Runs the whole domain on `stream` using caller-provided scratch (see bem3_scratch_bytes).
+// Returns 0, or a negative code (see bem3_qd2_b200.h).
+int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, size_t scratch_bytes, int rows_per_chunk,
+                      int* d_status, cudaStream_t st, AssembleStats* stats)
+{
+  if (ensure_tables() != 0) return BEM3_ERR_CUDA;
+  const int ne = A.ne;
+  const int nrows = 4 * ne;
+  if (rows_per_chunk <= 0 || rows_per_chunk > nrows) rows_per_chunk = nrows;
+  if (bem3_scratch_bytes(ne, rows_per_chunk) > scratch_bytes) return BEM3_ERR_SCRATCH;
+  char* base = (char*)scratch;
+  double3* Fself = (double3*)base;
+  size_t off = ((size_t)nrows * sizeof(double3) + 255) & ~(size_t)255;
+  unsigned* gh_count = (unsigned*)(base + off);
+  off += 256;
+  double3* Fp = (double3*)(base + off);
+  off += (((size_t)rows_per_chunk * ne * sizeof(double3)) + 255) & ~(size_t)255;
+  unsigned* gh_list = (unsigned*)(base + off);
+  unsigned gh_cap = (unsigned)((size_t)rows_per_chunk * ne / 8 + 4096);
+
+  const size_t N = (size_t)nrows;
+  if (cudaMemsetAsync(A.G, 0, N * N * 16, st) != cudaSuccess) return BEM3_ERR_CUDA;
+  if (cudaMemsetAsync(A.H, 0, N * N * 16, st) != cudaSuccess) return BEM3_ERR_CUDA;
+  if (A.dG && cudaMemsetAsync(A.dG, 0, 2 * N * N * 16, st) != cudaSuccess) return BEM3_ERR_CUDA;
+  if (A.dH && cudaMemsetAsync(A.dH, 0, 2 * N * N * 16, st) != cudaSuccess) return BEM3_ERR_CUDA;
+  if (A.dF && cudaMemsetAsync(A.dF, 0, N * 3 * sizeof(double), st) != cudaSuccess) return BEM3_ERR_CUDA;
+  cudaMemsetAsync(Fself, 0, N * sizeof(double3), st);
+
+  int launches = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  const bool timing = stats && stats->time_kernels && A.periodic;
+  if (timing) { cudaEventCreate(&ev0); cudaEventCreate(&ev1); }
+  // self pairs
+  if (A.periodic) k_self_periodic<<<nrows, SELF_THREADS, 0, st>>>(A, *L, Fself, d_status);
+  else bem3_launch_self_interior(A, Fself, d_status, st);
+  launches++;
+
+  for (int r0 = 0; r0 < nrows; r0 += rows_per_chunk) {
+    int nr = (r0 + rows_per_chunk <= nrows) ? rows_per_chunk : nrows - r0;
+    long long p0 = (long long)r0 * ne, np = (long long)nr * ne;
+    cudaMemsetAsync(gh_count, 0, sizeof(unsigned), st);
+    if (A.periodic) {
+      long long threads = np * 32;
+      unsigned blocks = (unsigned)((threads + 255) / 256);
+      if (timing) cudaEventRecord(ev0, st);
+      k_reg_periodic<<<blocks, 256, 0, st>>>(A, *L, p0, np, Fp, gh_list, gh_count, gh_cap, d_status);
+      if (timing) {
+        cudaEventRecord(ev1, st);
+        cudaEventSynchronize(ev1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        stats->reg_periodic_ms += ms;
+        stats->reg_periodic_launches++;
+      }
+      k_gh_periodic<<<148 * 4, 256, 0, st>>>(A, *L, p0, Fp, gh_list, gh_count, d_status);
+    } else {
+      unsigned blocks = (unsigned)((np + 127) / 128);
+      k_reg_interior<<<blocks, 128, 0, st>>>(A, p0, np, Fp, gh_list, gh_count, gh_cap, d_status);
+      k_gh_interior<<<148 * 4, 256, 0, st>>>(A, p0, Fp, gh_list, gh_count);
+    }
+    k_rowsum<<<(nr * 32 + 255) / 256, 256, 0, st>>>(A, r0, nr, Fp, Fself);
+    launches += 3;
+    if (stats) {
+      unsigned c = 0;
+      cudaMemcpyAsync(&c, gh_count, sizeof c, cudaMemcpyDeviceToHost, st);
+      cudaStreamSynchronize(st);
+      stats->gh_pairs += c;
+    }
+  }
+  if (timing) { cudaEventDestroy(ev0); cudaEventDestroy(ev1); }
+  if (stats) stats->launches += launches;
+  if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
+  return 0;
+}

@@ -1,0 +1,37 @@
+// bem3_internal.h -- declarations shared by the CUDA translation units of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "qpgf.cuh"
+
+#include "bem3_qd2_b200.h"
+
+struct AssembleArgs {
+  const double* geo;  // [(Ne+1) * GEO_STRIDE] element geometry, id 0 unused
+  const int* sid;     // [ne] signed element ids of the domain (0-based positions)
+  int ne;             // elements seen by the domain
+  int did;            // domain id (0 = open, periodic region)
+  int periodic;       // 1: quasi-periodic Green's function (did 0 with ps == 1)
+  double kre, kim;    // wave number of the domain
+  double* G;          // [N][N] complex (N = 4 ne)
+  double* H;          // [N][N] complex
+  double* dG;         // [2N][N] complex
+  double* dH;         // [2N][N] complex
+  double* dF;         // [N][3]
+  unsigned long long* terms;  // optional device counter: lattice-sum terms of the regular periodic pairs
+};
+
+struct AssembleStats {
+  unsigned long long gh_pairs;   // near-singular pairs recomputed with the 64x64 rule
+  int launches;                  // kernels launched
+  int time_kernels;              // in: 1 = time the regular periodic kernel with CUDA events
+  double reg_periodic_ms;        // out: summed duration of k_reg_periodic launches
+  int reg_periodic_launches;     // out: number of k_reg_periodic launches
+};
+
+size_t bem3_scratch_bytes(int ne, int rows);
+int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, size_t scratch_bytes, int rows_per_chunk,
+                      int* d_status, cudaStream_t st, AssembleStats* stats);
+void bem3_launch_self_interior(const AssembleArgs& A, double3* Fself, int* d_status, cudaStream_t st);

@@ -1,0 +1,124 @@
+/*
+ * bem3_qd2_b200.h -- C ABI of the B200 (sm_100a) implementation of bem3_emf_qd2's
+ * boundary-integral hot path: the quasi-periodic Green's function (QPGF) and the
+ * element-quadrature assembly of the coefficient matrices.
+ *
+ * Every entry point takes plain pointers and sizes; no CUDA or framework types appear in the
+ * signatures (a stream is passed as `void *`, NULL = the default stream).  Return values are
+ * 0 on success or one of the negative BEM3_ERR_* codes below.  Arrays follow the reference's
+ * in-memory conventions (1-based element ids with slot 0 unused, row-major complex doubles
+ * stored as interleaved re/im pairs) so that a caller holding a DQD2 (d3qd2_src/d3qd2_elem.h:49-60)
+ * can pass its arrays after flattening.
+ */
+#ifndef BEM3_QD2_B200_H_
+#define BEM3_QD2_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BEM3_OK 0
+#define BEM3_ERR_ARG -1      /* invalid argument */
+#define BEM3_ERR_CUDA -2     /* CUDA failure (device memory, launch, copy) */
+#define BEM3_ERR_SCRATCH -3  /* scratch smaller than required */
+#define BEM3_ERR_LATTICE -4  /* degenerate lattice, det[d1 d2] == 0 */
+#define BEM3_ERR_SOLVE -5    /* singular system */
+/* Kernel status codes (returned as is): -11..-14 and -21..-24 are the QPGF failures of
+ * d3hm_qpgf_d2_v1 (qgf2_src/d3_qpgf_d2.h:112-123); -900 near-singular work-list overflow. */
+
+/* Quasi-periodic data, same field order and meaning as QPD2 (qgf2_src/d3_qpgf_d2.h:32-36). */
+typedef struct {
+  double k;        /* wave number of the open (periodic) region */
+  double vk[3];    /* incident wave vector; vk[0], vk[1] give the Bloch phase */
+  double vd1[2];   /* lattice vector d1 (z = 0) */
+  double vd2[2];   /* lattice vector d2 (z = 0) */
+} bem3_qpd2;
+
+/* Surface mesh in the reference's element-constant form (BOUD, d3qd2_src/d3qd2_elem.h:22-47),
+ * flattened, element ids 1..Ne with slot 0 unused:
+ *   cr  [(Ne+1)][3][4]  bilinear/linear map coefficients  (init_elem_const, d3qd2_setup.c:1139)
+ *   cw  [(Ne+1)][3][3]  normal-vector (Jacobian) coefficients
+ *   ren [(Ne+1)][4][3]  collocation node positions        (init_boundary_data, d3qd2_setup.c:1309)
+ *   wen [(Ne+1)][4][3]  normal vectors at the nodes
+ *   nv  [(Ne+1)]        vertices per element: 3 (triangle) or 4 (bilinear quad)            */
+typedef struct {
+  int Ne;
+  const double *cr;
+  const double *cw;
+  const double *ren;
+  const double *wen;
+  const int *nv;
+} bem3_mesh;
+
+/* ---------------------------------------------------------------------------------------------
+ * Green's function.
+ * Replaces d3hm_qpgf_d2_v1 (qgf2_src/d3_qpgf_d2.h:112, d3_qpgf_d2.c:124) for n points at once.
+ * r: [n][3] host array; out: [n][4] complex (qG, dqG/dx, dqG/dy, dqG/dz); ret: [n] codes as the
+ * reference (> 0 number of lattice terms, < 0 failure).  mode 0: the reference's v1 stop rules;
+ * mode 1: stop only when the rules of both d3hm_qpgf_d2_qG and d3hm_qpgf_d2_dqG
+ * (d3_qpgf_d2.h:125-126) are met.  Runs on the current CUDA device. */
+int bem3_qpgf(const bem3_qpd2 *qd, int n, const double *r, double *out, int *ret, int mode);
+
+/* Same with device-resident r / out / ret (pointers into device memory) on `stream`. */
+int bem3_qpgf_dev(const bem3_qpd2 *qd, int n, const double *r_dev, double *out_dev, int *ret_dev, int mode,
+                  void *stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Coefficient matrices of one domain.
+ * Replaces create_cmatrix_domain (d3qd2_src/d3qd2_solve_bieq.c:165-256): for every collocation
+ * node (t, tn) of the domain and every source element s it evaluates what the reference gets
+ * from q0_dcoef_bd_node_t2_cc (did 0, periodic; d3qd2_elem.c:830) or dcoef_bd_node_t2 (interior
+ * domains; d3qd2_elem.c:515) with PREC_DEF_BE = 2, and writes the matrices that the reference
+ * writes to its tmpG/tmpH/tmpdG/tmpdH/tmpdF files, in the same layout (N = 4 Ne_d):
+ *   G, H   [N][N] complex,  dG, dH [2N][N] complex,  dF [N][3] double.
+ * sid: [Ne_d] signed element ids of the domain (sb[did].sid[1..Ne_d]).  periodic: 1 when
+ * did == 0 and the problem is periodic (bd.ps == 1).  kre/kim: domain wave number kn[did].
+ * dG, dH or dF may be NULL to skip them.  Host pointers; the call is synchronous. */
+int bem3_assemble_domain(const bem3_mesh *mesh, const int *sid, int Ne_d, int did, int periodic,
+                         const bem3_qpd2 *qd, double kre, double kim, double *G, double *H, double *dG,
+                         double *dH, double *dF);
+
+/* Device-resident variant.  geo_dev: packed geometry from bem3_pack_geometry (uploaded by the
+ * caller); sid_dev: [Ne_d] ints; outputs in device memory.  The library allocates its scratch
+ * (bem3_assemble_scratch_bytes) with cudaMalloc on first use and keeps it for later calls. */
+int bem3_assemble_domain_dev(const double *geo_dev, int Ne, const int *sid_dev, int Ne_d, int did, int periodic,
+                             const bem3_qpd2 *qd, double kre, double kim, double *G_dev, double *H_dev,
+                             double *dG_dev, double *dH_dev, double *dF_dev, void *stream);
+
+/* Packs a bem3_mesh into the device geometry layout: (Ne+1) * bem3_geo_stride() doubles. */
+int bem3_geo_stride(void);
+int bem3_pack_geometry(const bem3_mesh *mesh, double *geo);
+
+/* Counters of the last assembly on this thread: near-singular (64x64 rule) pairs. */
+unsigned long long bem3_last_gh_pairs(void);
+
+/* Profiling counters of the last assembly on this thread.  Filled only after
+ * bem3_set_profiling(1) (which adds a per-warp term counter and CUDA-event timing of the
+ * regular periodic kernel); otherwise only gh_pairs and launches are set. */
+typedef struct {
+  unsigned long long gh_pairs;     /* pairs recomputed with the 64x64 near-singular rule */
+  unsigned long long qpgf_terms;   /* lattice-sum terms summed by the regular periodic kernel */
+  int launches;                    /* kernels launched by the call */
+  int reg_periodic_launches;       /* launches of the regular periodic kernel */
+  double reg_periodic_ms;          /* their summed duration (CUDA events) */
+} bem3_stats;
+void bem3_set_profiling(int on);
+int bem3_last_stats(bem3_stats *out);
+
+/* Measures the FP64 FMA throughput of the current device (TFLOP/s), the denominator of the
+ * FP64 roofline.  Runs a ~100 ms kernel. */
+double bem3_fp64_peak_tflops(void);
+
+/* Gauss-Legendre nodes and weights on [-1, 1] (the reference's gauleg, com_src/gauleg.c:3). */
+void bem3_gauss_legendre(int n, double *x, double *w);
+
+/* Library version string. */
+const char *bem3_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEM3_QD2_B200_H_ */

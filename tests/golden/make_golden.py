@@ -1,0 +1,121 @@
+"""Generates the golden fixtures in this directory from the reference (akohta/bem3_emf_qd2).
+
+Run in a checkout where the reference sources are present (default /root/reference) after
+``make -C oracle ref``.  Every array stored here comes from the reference's own code, compiled
+from its sources by oracle/Makefile and called through oracle/reforacle.py:
+
+  gauleg.npz    the Gauss-Legendre tables of gauleg (com_src/gauleg.c) for n = 12, 64
+  faddeeva.npz  Faddeeva_w (qgf2_src/Faddeeva.cc) at seeded points, relerr 1e-15
+  qpgf.npz      d3hm_qpgf_d2_v1 / _qG / _dqG (qgf2_src/d3_qpgf_d2.c) for 5 lattices
+  rows_*.npz    inputs of a sample problem shipped with the reference (read by the reference's
+                own readers) and complete rows of create_cmatrix_domain
+                (d3qd2_src/d3qd2_solve_bieq.c:165-256) for selected collocation elements.
+
+Usage: python tests/golden/make_golden.py [reference_dir]
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+sys.path.insert(0, REPO)
+
+from reforacle import RefOracle  # noqa: E402
+from bem3_emf_qd2_b200.dqd2 import load_inputs  # noqa: E402
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+
+
+def qpd_of(k, th, ph, d1, d2):
+    vk = [k * np.sin(th) * np.cos(ph), k * np.sin(th) * np.sin(ph), k * np.cos(th)]
+    if vk[0] == 0.0:
+        vk[0] = k * 1e-15
+    if vk[1] == 0.0:
+        vk[1] = k * 1e-15
+    return np.array([k, *vk, *d1, *d2])
+
+
+LATTICES = {
+    # config-1 lattice (square 1.0, n=1.33, lambda0=0.6328, near-normal incidence)
+    "square1_c1": qpd_of(2 * np.pi * 1.33 / 0.6328, 1e-4, 0.0, (1.0, 0.0), (0.0, 1.0)),
+    # the reference's verification lattice (hexagonal 2.0, lambda0=1, theta=0.2)
+    "hex2_veri": qpd_of(2 * np.pi * 1.33 / 1.0, 0.2, 0.0, (2.0, 0.0), (1.0, 1.7320508075688772)),
+    # config-3 lattice (hexagonal 0.9, n=1.0, lambda0=0.7, theta=10 deg)
+    "hex09_c3": qpd_of(2 * np.pi * 1.0 / 0.7, np.radians(10.0), 0.0, (0.9, 0.0), (0.45, 0.7794)),
+    # config-2 lattice (square 1.0, lambda0=0.532, theta=30 deg, phi=45 deg)
+    "square1_c2": qpd_of(2 * np.pi * 1.33 / 0.532, np.pi / 6, np.pi / 4, (1.0, 0.0), (0.0, 1.0)),
+    # analysis_sample3 lattice (hexagonal 0.75)
+    "hex075": qpd_of(2 * np.pi * 1.33 / 1.0, 0.2, 0.0, (0.75, 0.0), (0.375, 0.649519052838329)),
+}
+
+CASES = {
+    # name: (directory, mesh, {did: [1-based collocation elements]})
+    "sphere_m4": ("verification", "sphere_m4.msh", {0: [1, 200], 1: [1, 100]}),
+    "cone_m1": ("analysis_sample2", "cone_m1.msh", {0: [1, 300], 1: [5]}),
+    "sphere_m2": ("analysis_sample1", "sphere_m2.msh", {0: [7], 1: [11], 2: [3]}),
+}
+
+
+def gauleg_tables(o):
+    d = os.path.join(REF, "verification")
+    o.load(*[os.path.join(d, f) for f in ("ipw.txt", "periodicity_data.txt", "medium_data.txt", "sphere_m4.msh")])
+    g = o.geometry()
+    np.savez_compressed(os.path.join(HERE, "gauleg.npz"), x12=g["xli"], w12=g["wli"], x64=g["xhi"], w64=g["whi"])
+
+
+def main():
+    o = RefOracle()
+    gauleg_tables(o)
+    rng = np.random.default_rng(20261203)
+
+    # ---- Faddeeva -----------------------------------------------------------------------
+    z = np.concatenate([
+        rng.uniform(-12, 12, 3000) + 1j * rng.uniform(-10, 14, 3000),
+        rng.uniform(-6, 6, 1000) + 1j * 10 ** rng.uniform(-12, 0.5, 1000) * rng.choice([-1, 1], 1000),
+        rng.uniform(-0.5, 0.5, 500) + 1j * rng.uniform(-0.5, 0.5, 500),
+    ])
+    np.savez_compressed(os.path.join(HERE, "faddeeva.npz"), z=z, w=o.faddeeva(z))
+
+    # ---- QPGF -----------------------------------------------------------------------------
+    out = {}
+    for name, p in LATTICES.items():
+        r = np.concatenate([rng.uniform(-0.7, 0.7, (1200, 3)), rng.uniform(-0.04, 0.04, (300, 3)),
+                            np.c_[rng.uniform(-1.5, 1.5, (300, 2)), rng.uniform(-2.5, 2.5, (300, 1))]])
+        v1, rv1 = o.qpgf(r, p, "v1")
+        g, rg = o.qpgf(r, p, "qG")
+        d, rd = o.qpgf(r, p, "dqG")
+        out[name + "/qpd"] = p
+        out[name + "/r"] = r
+        out[name + "/v1"] = v1
+        out[name + "/ret_v1"] = rv1
+        out[name + "/qG"] = g[:, 0]
+        out[name + "/dqG"] = d
+    np.savez_compressed(os.path.join(HERE, "qpgf.npz"), **out)
+
+    # ---- rows of the assembly -----------------------------------------------------------
+    for name, (sub, msh, sel) in CASES.items():
+        d = os.path.join(REF, sub)
+        files = [os.path.join(d, f) for f in ("ipw.txt", "periodicity_data.txt", "medium_data.txt", msh)]
+        o.load(*files)
+        arr = load_inputs(*files)
+        rec = {"in/" + k: v for k, v in arr.items()}
+        for did, elems in sel.items():
+            for t in elems:
+                G, H, dG, dH, dF = o.assemble_rows(did, t, t)
+                rec[f"d{did}/t{t}/G"] = G
+                rec[f"d{did}/t{t}/H"] = H
+                if did > 0:
+                    rec[f"d{did}/t{t}/dG"] = dG
+                    rec[f"d{did}/t{t}/dH"] = dH
+                else:
+                    rec[f"d{did}/t{t}/dGdH_absmax"] = np.array(max(np.abs(dG).max(), np.abs(dH).max()))
+                rec[f"d{did}/t{t}/dF"] = dF
+                print(name, did, t, "done", flush=True)
+        np.savez_compressed(os.path.join(HERE, f"rows_{name}.npz"), **rec)
+
+
+if __name__ == "__main__":
+    main()

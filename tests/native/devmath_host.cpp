@@ -30,3 +30,53 @@ void hm_qpgf(int n, const double* r, const double* p, int mode, double* out, int
 }
 
 }
+
+#include "elem.cuh"
+
+extern "C" {
+
+// One regular (t != s) pair with the device element rules, evaluated serially on the host.
+// geo: packed geometry; td, sd: signed element ids; tn: collocation node; periodic: 1 for the
+// open domain; n: 12 (GL) or 64 (GH); p: QPD2 order; out: CC[9], dCz[9], dCe[9] (re/im pairs).
+// Returns 1 when the GL result asks for the near-singular rule, else 0.
+int hm_pair_regular(const double* geo, int td, int tn, int sd, int periodic, double kre, double kim,
+                    const double* p, int n, const double* x, const double* w, double* out)
+{
+  QPLattice L;
+  qp_lattice_init(L, p[0], p[1], p[2], p[4], p[5], p[6], p[7]);
+  Elem et, es;
+  load_elem(geo, td < 0 ? -td : td, et);
+  load_elem(geo, sd < 0 ? -sd : sd, es);
+  double vtz[3], vte[3];
+  node_tangents(et, tn, vtz, vte);
+  const double* rt = geo + (size_t)(td < 0 ? -td : td) * GEO_STRIDE + GEO_REN + tn * 3;
+  int npts = (es.nn == 4) ? n * n : 3 * n * n;
+  cplx CC[9], dCz[9], dCe[9];
+  if (periodic) {
+    AccP a;
+    accp_zero(a);
+    for (int q = 0; q < npts; q++) {
+      double z, e, wt;
+      rule_point(es.nn, n, x, w, q, z, e, wt);
+      accp_point(es, L, rt, vtz, vte, z, e, wt, a);
+    }
+    accp_finish(es, a, CC, dCz, dCe);
+  } else {
+    AccI a;
+    acci_zero(a);
+    for (int q = 0; q < npts; q++) {
+      double z, e, wt;
+      rule_point(es.nn, n, x, w, q, z, e, wt);
+      acci_point(es, mk(kre, kim), rt, vtz, vte, z, e, wt, a);
+    }
+    acci_finish(es, a, sd < 0, CC, dCz, dCe);
+  }
+  for (int i = 0; i < 9; i++) {
+    out[2 * i] = CC[i].re; out[2 * i + 1] = CC[i].im;
+    out[18 + 2 * i] = dCz[i].re; out[19 + 2 * i] = dCz[i].im;
+    out[36 + 2 * i] = dCe[i].re; out[37 + 2 * i] = dCe[i].im;
+  }
+  return needs_gh(dCz[8].re, dCe[8].re);
+}
+
+}

@@ -1,0 +1,162 @@
+"""CPU tests: the oracle against the committed golden vectors, the device math compiled for the
+host against the same vectors, the host set-up, and the C-ABI library's exported symbols."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import REPO, golden
+
+
+def _rel(a, b, floor=1e-300):
+    return np.abs(a - b) / np.maximum(np.abs(b), floor)
+
+
+# ---- golden vectors pin the reference oracle (when it was built here) ------------------------
+@pytest.mark.skipif(not os.path.exists(os.path.join(REPO, "oracle", "_ref", "libbem3ref.so")),
+                    reason="reference oracle not built in this checkout")
+def test_reference_oracle_reproduces_goldens():
+    from reforacle import RefOracle
+    o = RefOracle()
+    f = golden("faddeeva.npz")
+    assert np.array_equal(o.faddeeva(f["z"]), f["w"])
+    q = golden("qpgf.npz")
+    names = sorted({k.split("/")[0] for k in q.files})
+    for n in names:
+        out, ret = o.qpgf(q[n + "/r"][:300], q[n + "/qpd"], "v1")
+        assert np.array_equal(out, q[n + "/v1"][:300]) and np.array_equal(ret, q[n + "/ret_v1"][:300])
+
+
+# ---- device math compiled for the host ------------------------------------------------------
+def test_faddeeva_host_build(devmath_host):
+    f = golden("faddeeva.npz")
+    z = f["z"]
+    zz = np.ascontiguousarray(np.stack([z.real, z.imag], 1).ravel())
+    out = np.zeros_like(zz)
+    devmath_host.hm_faddeeva(len(z), zz.ctypes.data, out.ctypes.data)
+    w = out[0::2] + 1j * out[1::2]
+    # |w - w_ref| / |w_ref|: the reference itself targets 1e-15 relative error
+    assert np.max(np.abs(w - f["w"]) / np.abs(f["w"])) < 1e-13
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_qpgf_host_build(devmath_host, mode):
+    q = golden("qpgf.npz")
+    names = sorted({k.split("/")[0] for k in q.files})
+    for n in names:
+        r = np.ascontiguousarray(q[n + "/r"])
+        out = np.zeros(len(r) * 8)
+        ret = np.zeros(len(r), np.int32)
+        devmath_host.hm_qpgf(len(r), r.ctypes.data, np.ascontiguousarray(q[n + "/qpd"]).ctypes.data, mode,
+                             out.ctypes.data, ret.ctypes.data)
+        got = (out[0::2] + 1j * out[1::2]).reshape(-1, 4)
+        assert np.all(ret > 0)
+        if mode == 0:
+            # same stop rules as d3hm_qpgf_d2_v1: identical term counts at every point
+            assert np.array_equal(ret, q[n + "/ret_v1"]), n
+            ref = q[n + "/v1"]
+        else:
+            ref = np.c_[q[n + "/qG"], q[n + "/dqG"]]
+        scale = np.abs(ref).max(axis=1, keepdims=True)
+        assert np.max(np.abs(got - ref) / scale) < 1e-10, n
+
+
+def _pack(p):
+    geo = np.zeros((p.Ne + 1, 48))
+    geo[:, 0:12] = p.cr.reshape(-1, 12)
+    geo[:, 12:21] = p.cw.reshape(-1, 9)
+    geo[:, 21:33] = p.ren.reshape(-1, 12)
+    geo[:, 33:45] = p.wen.reshape(-1, 12)
+    geo[:, 45] = p.nv
+    return np.ascontiguousarray(geo)
+
+
+@pytest.mark.parametrize("case", ["sphere_m4", "cone_m1", "sphere_m2"])
+def test_regular_pairs_host_build(devmath_host, case):
+    """Regular (t != s) pairs of the golden rows, re-evaluated with the device element rules."""
+    from bem3_emf_qd2_b200.dqd2 import problem_from_arrays
+    import bem3_emf_qd2_b200 as B
+    g = golden(f"rows_{case}.npz")
+    p = problem_from_arrays({k[3:]: g[k] for k in g.files if k.startswith("in/")})
+    geo = _pack(p)
+    qpd = np.array([p.qpd["k"], *p.qpd["vk"], *p.qpd["vd1"], *p.qpd["vd2"]])
+    xl, wl = _gl(12)
+    xh, wh = _gl(64)
+    rng = np.random.default_rng(7)
+    keys = [k for k in g.files if k.endswith("/G") and k.startswith("d")]
+    for key in keys:
+        did = int(key.split("/")[0][1:])
+        t = int(key.split("/")[1][1:])
+        G, H = g[key], g[key.replace("/G", "/H")]
+        ne = len(p.sid[did])
+        td = int(p.sid[did][t - 1])
+        for s in rng.choice(np.arange(1, ne + 1), size=12, replace=False):
+            if s == t:
+                continue
+            sd = int(p.sid[did][s - 1])
+            for tn in range(p.nv[abs(td)]):
+                out = np.zeros(54)
+                k = complex(p.kn[did])
+                args = [geo.ctypes.data, td, tn, sd, 1 if did == 0 else 0, k.real, k.imag, qpd.ctypes.data]
+                gh = devmath_host.hm_pair_regular(*args, 12, xl.ctypes.data, wl.ctypes.data, out.ctypes.data)
+                if gh:
+                    devmath_host.hm_pair_regular(*args, 64, xh.ctypes.data, wh.ctypes.data, out.ctypes.data)
+                c = out[0::2] + 1j * out[1::2]
+                ref_g = G[tn, 4 * (s - 1):4 * s]
+                ref_h = H[tn, 4 * (s - 1):4 * s]
+                sc = max(np.abs(ref_g).max(), np.abs(ref_h).max())
+                assert np.abs(c[0:4] - ref_g).max() < 1e-12 * sc
+                assert np.abs(c[4:8] - ref_h).max() < 1e-12 * sc
+
+
+def _gl(n):
+    """The library's Gauss-Legendre tables (the ones uploaded to the device)."""
+    import bem3_emf_qd2_b200 as B
+    x, w = B.gauss_legendre(n)
+    return np.ascontiguousarray(x), np.ascontiguousarray(w)
+
+
+# ---- host set-up mirrors the reference's readers ----------------------------------------------
+def test_problem_setup_shapes():
+    from bem3_emf_qd2_b200.dqd2 import problem_from_arrays
+    g = golden("rows_sphere_m2.npz")
+    p = problem_from_arrays({k[3:]: g[k] for k in g.files if k.startswith("in/")})
+    assert p.MN == 2 and p.Ne == 1086 and p.NN == 4344
+    assert [len(s) for s in p.sid] == [600, 486, 1086]
+    # every element appears once in its main and once in its sub domain
+    assert sum(len(s) for s in p.sid) == 2 * p.Ne
+
+
+# ---- the C ABI ----------------------------------------------------------------------------------
+def test_cabi_exports_every_declared_symbol():
+    so = os.path.join(REPO, "bem3_emf_qd2_b200", "_lib", "libbem3qd2.so")
+    if not os.path.exists(so):
+        pytest.fail("CUDA library not built (run __graft_entry__.build())")
+    hdrs = [os.path.join(REPO, "include", f) for f in os.listdir(os.path.join(REPO, "include")) if f.endswith(".h")]
+    declared = set()
+    for h in hdrs:
+        txt = open(h).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        declared |= set(re.findall(r"\b(bem3_\w+|solve_bieq|EH_\w+|mEMP_\w+)\s*\(", txt))
+    nm = subprocess.run(["nm", "-D", "--defined-only", so], capture_output=True, text=True, check=True).stdout
+    exported = {line.split()[-1] for line in nm.splitlines() if line.strip()}
+    missing = sorted(declared - exported)
+    assert not missing, missing
+
+
+def test_cabi_library_loads():
+    import bem3_emf_qd2_b200 as B
+    L = B.lib()
+    assert b"sm_100a" in L.bem3_version()
+
+
+def test_gauss_legendre_tables_match_reference():
+    """Near-singular pairs are sensitive to the last bit of the nodes: the device tables must be
+    the reference's gauleg output exactly."""
+    import bem3_emf_qd2_b200 as B
+    g = golden("gauleg.npz")
+    for n in (12, 64):
+        x, w = B.gauss_legendre(n)
+        assert np.array_equal(x, g[f"x{n}"]) and np.array_equal(w, g[f"w{n}"])
