@@ -24,7 +24,7 @@
 
 #include <vector>
 
-#include "elem.cuh"
+#include "self.cuh"
 #include "bem3_internal.h"
 
 // ------------------------------------------------------------------------------------------
@@ -345,7 +345,8 @@ __global__ void k_rowsum(AssembleArgs A, int row0, int nrows, const double3* Fp,
 
 // ==========================================================================================
 // Self pairs of the periodic domain (q0_bil_dcoef_bd_vt2_cc_DV q0_bil_dcoef_v2_cc.c:292-301 and
-// q0_lit_dcoef_bd_vt2_cc_DV q0_lit_dcoef_v2_cc.c:331-342).  One CTA per (t, tn).
+// q0_lit_dcoef_bd_vt2_cc_DV q0_lit_dcoef_v2_cc.c:331-342).  One CTA per (t, tn); the point loop
+// and the combination are self_per_points / self_per_combine (self.cuh).
 #define SELF_THREADS 256
 __global__ void __launch_bounds__(SELF_THREADS, 1) k_self_periodic(AssembleArgs A, QPLattice L, double3* Fself, int* status)
 {
@@ -353,66 +354,12 @@ __global__ void __launch_bounds__(SELF_THREADS, 1) k_self_periodic(AssembleArgs 
   __shared__ int serr[SELF_THREADS / 32];
   const int row = blockIdx.x;
   const int t = row >> 2, tn = row & 3;
-  const int sd = A.sid[t];
-  const int at = abs(sd);
-  Elem e;
-  load_elem(A.geo, at, e);
-  if (tn == 3 && e.nn == 3) return;
-  const double zt = node_zeta(e.nn, tn), et = node_eta(e.nn, tn);
-  PolarSet P;
-  polar_setup(e.nn, zt, et, P);
-  const int npts = P.nsub * 128 * 12;
-  cplx G[4], H[4];
-  for (int i = 0; i < 4; i++) { G[i] = mk(0, 0); H[i] = mk(0, 0); }
-  int err = 0;
-  for (int k = threadIdx.x; k < npts; k += blockDim.x) {
-    int ir = k % 12;
-    int tq = k / 12;
-    int j = tq >> 7, m2 = tq & 127;
-    double theta, wt;
-    polar_theta(P, j, m2, c_xh, c_wh, theta, wt);
-    double rm = polar_rm(P, j, theta);
-    double cth = cos(theta), sth = sin(theta);
-    double r = 0.5 * rm * (c_xl[ir] + 1.0);
-    double w = wt * 0.5 * rm * c_wl[ir];
-    double zeta = r * cth + zt, eta = r * sth + et;
-    double vR[3], W[3], N[4];
-    if (e.nn == 4) {
-      double K[3];
-      bil_K(e, zt, et, r, cth, sth, K);
-      for (int i = 0; i < 3; i++) {
-        vR[i] = r * K[i];
-        W[i] = e.cw[i][0] + e.cw[i][1] * zeta + e.cw[i][2] * eta;
-      }
-      bil_N4(zeta, eta, N);
-    } else {
-      for (int i = 0; i < 3; i++) {
-        vR[i] = r * (e.cr[i][1] * cth + e.cr[i][2] * sth);
-        W[i] = e.cw[i][0];
-      }
-      lit_N3(zeta, eta, N);
-      N[3] = 0.0;
-    }
-    QPVal g;
-    int e2 = qpgf_eval<QP_BOTH>(L, vR, g);
-    if (e2 < 0) err = e2;
-    double aW = (e.nn == 4) ? vnorm3(W) : 1.0;
-    cplx gw = g.G * (w * aW * r);
-    cplx hw = (g.dG[0] * W[0] + g.dG[1] * W[1] + g.dG[2] * W[2]) * (w * r);
-    for (int i = 0; i < 4; i++) { G[i] += gw * N[i]; H[i] += hw * N[i]; }
-  }
-  // curved quads: F at the node and at the four finite-difference neighbours
-  double Fv[5] = {0, 0, 0, 0, 0};
-  if (e.nn == 4 && !bil_is_plane(e)) {
-    const double h = EL_CDFH;
-    const double cz[5] = {zt, zt + h, zt - h, zt, zt};
-    const double ce[5] = {et, et, et, et + h, et - h};
-    for (int c = 0; c < 5; c++) Fv[c] = bil_self_F(e, cz[c], ce[c], c_xl, c_wl, c_xh, c_wh, threadIdx.x, blockDim.x);
-  }
+  SelfInfo S;
+  self_setup(A.geo, abs(A.sid[t]), tn, mk(0.0, 0.0), S);
+  if (tn == 3 && S.e.nn == 3) return;
   double v[24];
-  for (int i = 0; i < 4; i++) { v[2 * i] = G[i].re; v[2 * i + 1] = G[i].im; v[8 + 2 * i] = H[i].re; v[9 + 2 * i] = H[i].im; }
-  for (int c = 0; c < 5; c++) v[16 + c] = Fv[c];
-  v[21] = v[22] = v[23] = 0.0;
+  for (int i = 0; i < 24; i++) v[i] = 0.0;
+  int err = self_per_points(S, L, c_xl, c_wl, c_xh, c_wh, threadIdx.x, blockDim.x, v);
   warp_sum_arr<24>(v);
   err = warp_min_i(err);
   int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -425,25 +372,7 @@ __global__ void __launch_bounds__(SELF_THREADS, 1) k_self_periodic(AssembleArgs 
   if (lane != 0) return;
   record_status(status, e3);
   cplx CC[9], dCz[9], dCe[9];
-  for (int i = 0; i < 9; i++) { CC[i] = mk(0, 0); dCz[i] = mk(0, 0); dCe[i] = mk(0, 0); }
-  if (e.nn == 4) {
-    for (int i = 0; i < 4; i++) { CC[i] = mk(v[2 * i], v[2 * i + 1]); CC[i + 4] = mk(v[8 + 2 * i], v[9 + 2 * i]); }
-    double bdC = e.cr[0][1] * e.cw[0][2] + e.cr[1][1] * e.cw[1][2] + e.cr[2][1] * e.cw[2][2];
-    double s = EL_I_FP * bdC;
-    CC[8] = mk(v[16] * s, 0);
-    // dF/dt by central differences (q0_bil_dcoef_bd_tz0_cc_DV :336-362, te0 :364-390)
-    double Tz[3], Te[3];
-    for (int i = 0; i < 3; i++) { Tz[i] = e.cr[i][1] + e.cr[i][3] * et; Te[i] = e.cr[i][2] + e.cr[i][3] * zt; }
-    dCz[8] = mk(1.0 / vnorm3(Tz) * (v[17] * s - v[18] * s) / (2.0 * EL_CDFH), 0);
-    dCe[8] = mk(1.0 / vnorm3(Te) * (v[19] * s - v[20] * s) / (2.0 * EL_CDFH), 0);
-  } else {
-    double V[3] = {e.cw[0][0], e.cw[1][0], e.cw[2][0]};
-    double aV = vnorm3(V);
-    for (int i = 0; i < 3; i++) {
-      CC[i] = mk(v[2 * i], v[2 * i + 1]) * (2.0 / (3.0 * EL_SQ3) * aV);
-      CC[i + 4] = mk(v[8 + 2 * i], v[9 + 2 * i]) * (2.0 / (3.0 * EL_SQ3));
-    }
-  }
+  self_per_combine(S, v, CC, dCz, dCe);
   store_pair(A, row, t, CC, dCz, dCe, Fself, row, -1);
 }
 

@@ -68,11 +68,20 @@ BEM_CONST double fad_taylor[24] = {  // 1 / Gamma(n/2 + 1)
 #define FAD_H_OVER_PI 1.3369015219719208205e-1
 #define FAD_INV_SQRTPI 5.6418958354775628695e-1
 
+#if defined(BEM_TERM_STATS) && !defined(__CUDACC__)
+// host-only instrumentation for the term-mix study (never defined in the CUDA library build)
+extern unsigned long long bem_stat_w[3];
+#define BEM_STAT_W(i) (bem_stat_w[i]++)
+#else
+#define BEM_STAT_W(i) ((void)0)
+#endif
+
 // w(z) for Im z >= 0 (upper half plane incl. the real axis).
 BEM_HD cplx faddeeva_w_upper(double x, double y)
 {
   const double r2 = x * x + y * y;
   if (r2 >= 64.0) {
+    BEM_STAT_W(0);
     // continued fraction, 20 levels, bottom-up
     cplx z = mk(x, y);
     cplx t = z;
@@ -82,6 +91,7 @@ BEM_HD cplx faddeeva_w_upper(double x, double y)
     return mk(-FAD_INV_SQRTPI * q.im, FAD_INV_SQRTPI * q.re);  // i q / sqrt(pi)
   }
   if (r2 < 0.25) {
+    BEM_STAT_W(1);
     // Maclaurin series in (i z), Horner form
     cplx iz = mk(-y, x);
     cplx s = mk(fad_taylor[23], 0.0);
@@ -89,6 +99,7 @@ BEM_HD cplx faddeeva_w_upper(double x, double y)
     for (int n = 22; n >= 0; n--) s = s * iz + mk(fad_taylor[n], 0.0);
     return s;
   }
+  BEM_STAT_W(2);
   // trapezoid + pole correction; pick the node set farther from x
   const double u = fabs(x) * (1.0 / FAD_H);
   const double frac = u - floor(u);

@@ -73,11 +73,19 @@ BEM_HD int qp_diff(cplx v, cplx s, double eps)  // d3hm_sf_diff_z: |v| negligibl
   return (fabs(v.re) <= fabs(s.re) * QP_EFS * eps) && (fabs(v.im) <= fabs(s.im) * QP_EFS * eps);
 }
 
+#if defined(BEM_TERM_STATS) && !defined(__CUDACC__)
+extern unsigned long long bem_stat_t[5];  // real-space, spectral prop., spectral evan., FD prop., FD evan.
+#define BEM_STAT_T(i) (bem_stat_t[i]++)
+#else
+#define BEM_STAT_T(i) ((void)0)
+#endif
+
 // ---------------------------------------------------------------------------------------------
 // Ewald real-space term (d3_qpgf_d2.c:1814-1838).  F and dF[3] (dF[2] still lacks the
 // factor -z/(4 pi) that the sum applies at the end).
 BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1, int l2, cplx& F, cplx* dF)
 {
+  BEM_STAT_T(0);
   double Rl0 = (double)l1 * L.d1x + (double)l2 * L.d2x;
   double Rl1 = (double)l1 * L.d1y + (double)l2 * L.d2y;
   double px = r[0] + Rl0, py = r[1] + Rl1;
@@ -106,6 +114,7 @@ BEM_HD int qp_ew2_term(const QPLattice& L, const double* r, double veps, int n1,
   double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
   cplx ce = expi(an0 * r[0] + an1 * r[1]);
   if (bn2 > 0.0) {
+    BEM_STAT_T(1);
     double bn = sqrt(bn2);
     double azve = r[2] / (2.0 * veps);
     double ef = exp(bn2 * veps * veps - azve * azve);
@@ -119,6 +128,7 @@ BEM_HD int qp_ew2_term(const QPLattice& L, const double* r, double veps, int n1,
     dF[2] = 2.0 * (ce * mk(ef * w.re - ff.re, -ff.im));
     return 0;
   } else if (bn2 < 0.0) {
+    BEM_STAT_T(2);
     double bn = sqrt(-bn2);
     double azve = r[2] / (2.0 * veps);
     double ebz = exp(bn * r[2]);
@@ -141,6 +151,7 @@ BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx&
   double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
   double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
   if (bn2 > 0.0) {
+    BEM_STAT_T(3);
     double bn = sqrt(bn2);
     dF[2] = expi(an0 * r[0] + an1 * r[1] + bn * fabs(r[2]));
     F = dF[2] * (1.0 / bn);
@@ -148,6 +159,7 @@ BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx&
     dF[1] = F * an1;
     return 0;
   } else if (bn2 < 0.0) {
+    BEM_STAT_T(4);
     double bn = sqrt(-bn2);
     dF[2] = expi(an0 * r[0] + an1 * r[1]) * exp(-bn * fabs(r[2]));
     F = mul_mi(dF[2] * (1.0 / bn));

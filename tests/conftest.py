@@ -38,6 +38,9 @@ def devmath_host():
     lib.hm_qpgf.argtypes = [i, vp, vp, i, vp, vp]
     lib.hm_pair_regular.argtypes = [vp, i, i, i, i, d, d, vp, i, vp, vp, vp]
     lib.hm_pair_regular.restype = i
+    lib.hm_self_interior.argtypes = [vp, i, i, d, d, vp, vp, vp, vp, vp]
+    lib.hm_self_periodic.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp]
+    lib.hm_self_periodic.restype = i
     return lib
 
 

@@ -80,3 +80,55 @@ int hm_pair_regular(const double* geo, int td, int tn, int sd, int periodic, dou
 }
 
 }
+
+#include "self.cuh"
+
+extern "C" {
+
+// Interior self pair (t == s) evaluated serially with the device pieces; out as hm_pair_regular.
+void hm_self_interior(const double* geo, int sd, int tn, double kre, double kim, const double* xl, const double* wl,
+                      const double* xh, const double* wh, double* out)
+{
+  SelfInfo S;
+  self_setup(geo, sd < 0 ? -sd : sd, tn, mk(kre, kim), S);
+  double R[4][SELF_NV];
+  for (int p = 0; p < 4; p++) for (int i = 0; i < SELF_NV; i++) R[p][i] = 0.0;
+  self_int_piece1(S, xl, wl, xh, wh, 0, 1, R[0]);
+  self_int_piece2(S, xh, wh, 0, 1, R[1]);
+  self_int_piece3(S, xl, wl, xh, wh, 0, 1, R[2]);
+  self_int_piece4(S, xl, wl, xh, wh, 0, 1, R[3]);
+  cplx CC[9], dCz[9], dCe[9];
+  self_int_combine(S, R[0], R[1], R[2], R[3], sd < 0, CC, dCz, dCe);
+  for (int i = 0; i < 9; i++) {
+    out[2 * i] = CC[i].re; out[2 * i + 1] = CC[i].im;
+    out[18 + 2 * i] = dCz[i].re; out[19 + 2 * i] = dCz[i].im;
+    out[36 + 2 * i] = dCe[i].re; out[37 + 2 * i] = dCe[i].im;
+  }
+}
+
+}
+
+extern "C" {
+
+// Periodic self pair evaluated serially with the device routine; p: QPD2 order.
+int hm_self_periodic(const double* geo, int sd, int tn, const double* p, const double* xl, const double* wl,
+                     const double* xh, const double* wh, double* out)
+{
+  QPLattice L;
+  qp_lattice_init(L, p[0], p[1], p[2], p[4], p[5], p[6], p[7]);
+  SelfInfo S;
+  self_setup(geo, sd < 0 ? -sd : sd, tn, mk(0.0, 0.0), S);
+  double v[24];
+  for (int i = 0; i < 24; i++) v[i] = 0.0;
+  int err = self_per_points(S, L, xl, wl, xh, wh, 0, 1, v);
+  cplx CC[9], dCz[9], dCe[9];
+  self_per_combine(S, v, CC, dCz, dCe);
+  for (int i = 0; i < 9; i++) {
+    out[2 * i] = CC[i].re; out[2 * i + 1] = CC[i].im;
+    out[18 + 2 * i] = dCz[i].re; out[19 + 2 * i] = dCz[i].im;
+    out[36 + 2 * i] = dCe[i].re; out[37 + 2 * i] = dCe[i].im;
+  }
+  return err;
+}
+
+}

@@ -160,3 +160,75 @@ def test_gauss_legendre_tables_match_reference():
     for n in (12, 64):
         x, w = B.gauss_legendre(n)
         assert np.array_equal(x, g[f"x{n}"]) and np.array_equal(w, g[f"w{n}"])
+
+
+# ---- the C restatement oracle (oracle/qpgf_oracle.c) is pinned to the reference's vectors -------
+def _port():
+    import ctypes as C
+    so = os.path.join(REPO, "oracle", "_build", "libqpgf_oracle.so")
+    if not os.path.exists(so):
+        subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "port"], check=True, capture_output=True)
+    L = C.CDLL(so)
+    L.or_faddeeva_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+    L.or_qpgf_batch.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    return L
+
+
+def test_restatement_oracle_pinned_to_reference_vectors():
+    L = _port()
+    f = golden("faddeeva.npz")
+    z = f["z"]
+    zz = np.ascontiguousarray(np.stack([z.real, z.imag], 1).ravel())
+    o = np.zeros_like(zz)
+    L.or_faddeeva_batch(len(z), zz.ctypes.data, o.ctypes.data)
+    assert np.max(np.abs(o[0::2] + 1j * o[1::2] - f["w"]) / np.abs(f["w"])) < 1e-13
+    q = golden("qpgf.npz")
+    for n in sorted({k.split("/")[0] for k in q.files}):
+        r = np.ascontiguousarray(q[n + "/r"])
+        out = np.zeros(len(r) * 8)
+        ret = np.zeros(len(r), np.int32)
+        L.or_qpgf_batch(len(r), r.ctypes.data, np.ascontiguousarray(q[n + "/qpd"]).ctypes.data, out.ctypes.data,
+                        ret.ctypes.data)
+        got = (out[0::2] + 1j * out[1::2]).reshape(-1, 4)
+        ref = q[n + "/v1"]
+        assert np.array_equal(ret, q[n + "/ret_v1"]), n
+        assert np.max(np.abs(got - ref) / np.abs(ref).max(axis=1, keepdims=True)) < 1e-12, n
+
+
+@pytest.mark.parametrize("case", ["sphere_m4", "cone_m1", "sphere_m2"])
+def test_self_pairs_host_build(devmath_host, case):
+    """Self pairs (t == s) with the device polar / principal-value routines against the golden
+    rows' self blocks (G, H) -- periodic and interior, quads and triangles."""
+    from bem3_emf_qd2_b200.dqd2 import problem_from_arrays
+    g = golden(f"rows_{case}.npz")
+    p = problem_from_arrays({k[3:]: g[k] for k in g.files if k.startswith("in/")})
+    geo = _pack(p)
+    qpd = np.array([p.qpd["k"], *p.qpd["vk"], *p.qpd["vd1"], *p.qpd["vd2"]])
+    xl, wl = _gl(12)
+    xh, wh = _gl(64)
+    for key in [k for k in g.files if k.endswith("/G") and k.startswith("d")]:
+        did = int(key.split("/")[0][1:])
+        t = int(key.split("/")[1][1:])
+        sd = int(p.sid[did][t - 1])
+        for tn in range(p.nv[abs(sd)]):
+            out = np.zeros(54)
+            if did == 0:
+                rc = devmath_host.hm_self_periodic(geo.ctypes.data, sd, tn, qpd.ctypes.data, xl.ctypes.data,
+                                                   wl.ctypes.data, xh.ctypes.data, wh.ctypes.data, out.ctypes.data)
+                assert rc == 0
+            else:
+                k = complex(p.kn[did])
+                devmath_host.hm_self_interior(geo.ctypes.data, sd, tn, k.real, k.imag, xl.ctypes.data, wl.ctypes.data,
+                                              xh.ctypes.data, wh.ctypes.data, out.ctypes.data)
+            c = out[0::2] + 1j * out[1::2]
+            cols = slice(4 * (t - 1), 4 * t)
+            ref_g = g[key][tn, cols]
+            ref_h = g[key.replace("/G", "/H")][tn, cols].copy()
+            ref_h[tn] -= g[key.replace("/G", "/dF")][tn, 0]  # the row sum (1+)F sits on the diagonal
+            sc = max(np.abs(ref_g).max(), np.abs(ref_h).max())
+            assert np.abs(c[0:4] - ref_g).max() < 1e-11 * sc, (case, did, t, tn)
+            assert np.abs(c[4:8] - ref_h).max() < 1e-11 * sc, (case, did, t, tn)
+            if did > 0:
+                for name, dc in (("dG", c[9:13]), ("dH", c[13:17])):
+                    ref = g[key.replace("/G", "/" + name)][2 * tn, cols]
+                    assert np.abs(dc - ref).max() < 1e-11 * max(np.abs(ref).max(), 1e-300), (case, did, t, tn, name)
