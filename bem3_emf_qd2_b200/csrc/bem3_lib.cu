@@ -3,3 +3,4 @@
 #include "assemble.cu"
 #include "self_interior.cu"
 #include "capi.cu"
+#include "solve.cu"

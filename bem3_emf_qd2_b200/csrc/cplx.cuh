@@ -9,8 +9,10 @@
 
 #if defined(__CUDACC__)
 #define BEM_HD __host__ __device__ __forceinline__
+#define BEM_HD_NOINLINE __host__ __device__ __noinline__
 #else
 #define BEM_HD static inline
+#define BEM_HD_NOINLINE static
 #endif
 
 struct cplx {

@@ -76,8 +76,10 @@ extern unsigned long long bem_stat_w[3];
 #define BEM_STAT_W(i) ((void)0)
 #endif
 
-// w(z) for Im z >= 0 (upper half plane incl. the real axis).
-BEM_HD cplx faddeeva_w_upper(double x, double y)
+// w(z) for Im z >= 0 (upper half plane incl. the real axis).  Kept out of line and not unrolled:
+// one small copy serves every call site, which keeps the lattice-sum kernels inside the
+// instruction cache.
+BEM_HD_NOINLINE cplx faddeeva_w_upper(double x, double y)
 {
   const double r2 = x * x + y * y;
   if (r2 >= 64.0) {
@@ -85,7 +87,7 @@ BEM_HD cplx faddeeva_w_upper(double x, double y)
     // continued fraction, 20 levels, bottom-up
     cplx z = mk(x, y);
     cplx t = z;
-#pragma unroll
+#pragma unroll 1
     for (int n = 20; n >= 1; n--) t = z - (0.5 * n) * crecip(t);
     cplx q = crecip(t);
     return mk(-FAD_INV_SQRTPI * q.im, FAD_INV_SQRTPI * q.re);  // i q / sqrt(pi)
@@ -95,7 +97,7 @@ BEM_HD cplx faddeeva_w_upper(double x, double y)
     // Maclaurin series in (i z), Horner form
     cplx iz = mk(-y, x);
     cplx s = mk(fad_taylor[23], 0.0);
-#pragma unroll
+#pragma unroll 1
     for (int n = 22; n >= 0; n--) s = s * iz + mk(fad_taylor[n], 0.0);
     return s;
   }
@@ -108,11 +110,11 @@ BEM_HD cplx faddeeva_w_upper(double x, double y)
   const cplx z2 = z * z;
   cplx s = mk(0.0, 0.0);
   if (use_full) {
-#pragma unroll
+#pragma unroll 1
     for (int n = FAD_NFULL - 1; n >= 1; n--) s += fad_cfull[n] * crecip(mk(z2.re - fad_tfull[n], z2.im));
     s = (2.0 * s) * z + crecip(z);
   } else {
-#pragma unroll
+#pragma unroll 1
     for (int n = FAD_NHALF - 1; n >= 0; n--) s += fad_chalf[n] * crecip(mk(z2.re - fad_thalf[n], z2.im));
     s = (2.0 * s) * z;
   }

@@ -56,6 +56,7 @@ struct QPLattice {
   double bN, bNp, bNm;   // method selection (d3_qpgf_d2.c:135-155)
   int ew_only;           // 1 when bNp>0 || bNm>0 (always Ewald)
   int nc1;               // round(k||.d1 / 2 pi)
+  cplx eb2;              // e^{i k||.d2}: Bloch phase step along d2 in the real-space sum
 };
 
 struct QPVal {
@@ -82,8 +83,9 @@ extern unsigned long long bem_stat_t[5];  // real-space, spectral prop., spectra
 
 // ---------------------------------------------------------------------------------------------
 // Ewald real-space term (d3_qpgf_d2.c:1814-1838).  F and dF[3] (dF[2] still lacks the
-// factor -z/(4 pi) that the sum applies at the end).
-BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1, int l2, cplx& F, cplx* dF)
+// factor -z/(4 pi) that the sum applies at the end).  ce = e^{i k||.R_l} is supplied by the
+// caller, which advances it along a row by one complex multiply per term instead of a sincos.
+BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1, int l2, cplx ce, cplx& F, cplx* dF)
 {
   BEM_STAT_T(0);
   double Rl0 = (double)l1 * L.d1x + (double)l2 * L.d2x;
@@ -94,7 +96,6 @@ BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1
   double ke = L.k * veps;
   double i_ve = 1.0 / veps;
   double rl_2e = rl * 0.5 * i_ve;
-  cplx ce = expi(L.vkx * Rl0 + L.vky * Rl1);
   double ef = exp(ke * ke - rl_2e * rl_2e);
   cplx w = faddeeva_w(ke, rl_2e);
   double cfr = i_rl * i_rl * ef * (i_rl * w.re - L.k * w.im + i_ve * QP_INV_SQRTPI);
@@ -106,13 +107,12 @@ BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1
 }
 
 // Ewald spectral term (d3_qpgf_d2.c:1965-2009).  Returns 0 propagating, 1 evanescent,
-// -3 when beta_n == 0 exactly.
-BEM_HD int qp_ew2_term(const QPLattice& L, const double* r, double veps, int n1, int n2, cplx& F, cplx* dF)
+// -3 when beta_n == 0 exactly.  ce = e^{i a_n.r} comes from the caller's row recurrence.
+BEM_HD int qp_ew2_term(const QPLattice& L, const double* r, double veps, int n1, int n2, cplx ce, cplx& F, cplx* dF)
 {
   double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
   double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
   double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
-  cplx ce = expi(an0 * r[0] + an1 * r[1]);
   if (bn2 > 0.0) {
     BEM_STAT_T(1);
     double bn = sqrt(bn2);
@@ -145,7 +145,8 @@ BEM_HD int qp_ew2_term(const QPLattice& L, const double* r, double veps, int n1,
 }
 
 // Fourier-domain term (d3_qpgf_d2.c:856-885).  Returns 0 propagating, 1 evanescent, -2 if beta_n==0.
-BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx& F, cplx* dF)
+// ph = e^{i a_n.r} comes from the caller's row recurrence.
+BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx ph, cplx& F, cplx* dF)
 {
   double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
   double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
@@ -153,7 +154,7 @@ BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx&
   if (bn2 > 0.0) {
     BEM_STAT_T(3);
     double bn = sqrt(bn2);
-    dF[2] = expi(an0 * r[0] + an1 * r[1] + bn * fabs(r[2]));
+    dF[2] = ph * expi(bn * fabs(r[2]));
     F = dF[2] * (1.0 / bn);
     dF[0] = F * an0;
     dF[1] = F * an1;
@@ -161,7 +162,7 @@ BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx&
   } else if (bn2 < 0.0) {
     BEM_STAT_T(4);
     double bn = sqrt(-bn2);
-    dF[2] = expi(an0 * r[0] + an1 * r[1]) * exp(-bn * fabs(r[2]));
+    dF[2] = ph * exp(-bn * fabs(r[2]));
     F = mul_mi(dF[2] * (1.0 / bn));
     dF[0] = F * an0;
     dF[1] = F * an1;
@@ -171,44 +172,66 @@ BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx&
 }
 
 // ---------------------------------------------------------------------------------------------
+// The three lattice sums below follow the reference's loop nests (rows outermost: the centre row,
+// then rows +1, +2, ... until the row rule stops them, then rows -1, -2, ...; inside a row the
+// centre term, then the +side and the -side until the term rule stops each) and its stop rules,
+// but each is written as ONE flat loop that evaluates exactly one term per iteration and then
+// advances a small (row, side, offset) state.  On the GPU, lanes of a warp that follow different
+// paths through the nest re-converge at every term instead of at the end of each inner loop, and
+// each term function has a single call site (small code, no instruction-cache thrash).
+
 // Ewald real-space sum (d3_qpgf_d2.c:1714-1812).  Returns the number of terms or -1.
 template <int MODE>
 BEM_HD int qp_ew1_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
 {
-  int cc = 0;
   S = mk(0, 0); dS[0] = mk(0, 0); dS[1] = mk(0, 0); dS[2] = mk(0, 0);
-  cplx F, dF[3];
-  // l1 = 0, then l1 > 0, then l1 < 0
-  for (int dir = 0; dir < 3; dir++) {
-    int l1start = (dir == 0) ? 0 : (dir == 1 ? 1 : -1);
-    int step = (dir == 2) ? -1 : 1;
-    int l1;
-    for (l1 = l1start; (dir == 0) ? (l1 == 0) : (l1 * step < QP_EW_LIMIT); l1 += step) {
-      cplx oS = S, od0 = dS[0], od1 = dS[1];
-      // one row over l2 (d3_qpgf_d2.c:1762-1812)
-      int lc = -(int)round(((r[0] + (double)l1 * L.d1x) * L.d2x + (r[1] + (double)l1 * L.d1y) * L.d2y) / L.ad22);
-      qp_ew1_term(L, r, veps, l1, lc, F, dF);
-      S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
-      cc++;
-      for (int side = 0; side < 2; side++) {
-        int s2 = side ? -1 : 1;
-        int l2;
-        for (l2 = lc + s2; (l2 - lc) * s2 < QP_EW_LIMIT; l2 += s2) {
-          qp_ew1_term(L, r, veps, l1, l2, F, dF);
-          S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
-          cc++;
-          bool stop = qp_diff(F, S, eps);
-          if (MODE == QP_BOTH) stop = stop && qp_diff(dF[0], dS[0], eps) && qp_diff(dF[1], dS[1], eps);
-          if (stop) break;
-        }
-        if ((l2 - lc) * s2 >= QP_EW_LIMIT) return -1;
-      }
-      if (dir == 0) break;
-      bool stop = qp_comp(S, oS, eps);
-      if (MODE == QP_BOTH) stop = stop && qp_comp(dS[0], od0, eps) && qp_comp(dS[1], od1, eps);
-      if (stop) break;
+  cplx oS = S, od0 = S, od1 = S;
+  int cc = 0, dir = 0, l1 = 0, side = -1, off = 0;
+  int lc = -(int)round((r[0] * L.d2x + r[1] * L.d2y) / L.ad22);
+  cplx ce0 = expi(L.vkx * ((double)lc * L.d2x) + L.vky * ((double)lc * L.d2y));
+  cplx ce = ce0;
+  for (;;) {
+    const int l2 = lc + (side == 1 ? -off : off);
+    cplx F, dF[3];
+    qp_ew1_term(L, r, veps, l1, l2, ce, F, dF);
+    S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
+    cc++;
+    bool row_done = false;
+    if (side < 0) {
+      side = 0; off = 1; ce = ce0 * L.eb2;
+      continue;
     }
-    if (dir != 0 && l1 * step >= QP_EW_LIMIT) return -1;
+    bool stop = qp_diff(F, S, eps);
+    if (MODE == QP_BOTH) stop = stop && qp_diff(dF[0], dS[0], eps) && qp_diff(dF[1], dS[1], eps);
+    if (stop) {
+      if (side == 0) { side = 1; off = 1; ce = ce0 * conj(L.eb2); continue; }
+      row_done = true;
+    } else {
+      if (off + 1 >= QP_EW_LIMIT) return -1;
+      off++;
+      ce = ce * (side == 0 ? L.eb2 : conj(L.eb2));
+    }
+    if (!row_done) continue;
+    // row finished: the row rule decides between the next row and the next direction
+    bool rstop = true;
+    if (dir != 0) {
+      rstop = qp_comp(S, oS, eps);
+      if (MODE == QP_BOTH) rstop = rstop && qp_comp(dS[0], od0, eps) && qp_comp(dS[1], od1, eps);
+    }
+    if (rstop) {
+      if (dir == 2) break;
+      dir++;
+      l1 = (dir == 1) ? 1 : -1;
+    } else {
+      l1 += (dir == 1) ? 1 : -1;
+      if (l1 >= QP_EW_LIMIT || l1 <= -QP_EW_LIMIT) return -1;
+    }
+    oS = S; od0 = dS[0]; od1 = dS[1];
+    lc = -(int)round(((r[0] + (double)l1 * L.d1x) * L.d2x + (r[1] + (double)l1 * L.d1y) * L.d2y) / L.ad22);
+    ce0 = expi(L.vkx * ((double)l1 * L.d1x + (double)lc * L.d2x) + L.vky * ((double)l1 * L.d1y + (double)lc * L.d2y));
+    ce = ce0;
+    side = -1;
+    off = 0;
   }
   const double f4p = 4.0 * QP_PI;
   S = mk(S.re / f4p, S.im / f4p);
@@ -218,110 +241,95 @@ BEM_HD int qp_ew1_sum(const QPLattice& L, const double* r, double veps, double e
   return cc;
 }
 
-// Ewald spectral sum (d3_qpgf_d2.c:1840-1963).  Returns the number of terms or -2 / -3.
-template <int MODE>
-BEM_HD int qp_ew2_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
+// Spectral sums share their row structure.  FD == 0: Ewald spectral sum (d3_qpgf_d2.c:1840-1963,
+// returns terms or -2 / -3); FD == 1: Fourier-domain sum (d3_qpgf_d2.c:745-854, returns terms or
+// -1 / -2 / -4).  Row rule of the Ewald sum applies only to rows without propagating orders
+// beyond the centre (the reference's flg).
+template <int MODE, int FD>
+BEM_HD int qp_spec_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
 {
-  int cc = 0;
+  if (FD && r[2] == 0.0) return -4;
+  const int LIMIT = FD ? QP_FD_LIMIT : QP_EW_LIMIT;
+  const int ELIM = FD ? -1 : -2;
   S = mk(0, 0); dS[0] = mk(0, 0); dS[1] = mk(0, 0); dS[2] = mk(0, 0);
-  cplx F, dF[3];
+  cplx oS = S, od2 = S;
   const int nc = L.nc1;
-  for (int dir = 0; dir < 3; dir++) {
-    int n1start = (dir == 0) ? nc : (dir == 1 ? nc + 1 : nc - 1);
-    int step = (dir == 2) ? -1 : 1;
-    int n1;
-    for (n1 = n1start; (dir == 0) ? (n1 == nc) : ((n1 - nc) * step < QP_EW_LIMIT); n1 += step) {
-      cplx oS = S, od2 = dS[2];
-      // one row over n2 (d3_qpgf_d2.c:1902-1963)
-      int nc2 = (int)round(-((-L.vkx + (double)n1 * L.g1x) * L.g2x + (-L.vky + (double)n1 * L.g1y) * L.g2y) / L.g22);
-      int flg = 0;
-      int e = qp_ew2_term(L, r, veps, n1, nc2, F, dF);
-      cc++;
-      if (e < 0) return e;
-      S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
-      for (int side = 0; side < 2; side++) {
-        int s2 = side ? -1 : 1;
-        int n2;
-        for (n2 = nc2 + s2; (n2 - nc2) * s2 < QP_EW_LIMIT; n2 += s2) {
-          e = qp_ew2_term(L, r, veps, n1, n2, F, dF);
-          cc++;
-          if (e < 0) return e;
-          S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
-          if (e > 0) {
-            bool stop = qp_diff(dF[2], dS[2], eps);
-            if (MODE == QP_BOTH) stop = stop && qp_diff(F, S, eps);
-            if (stop) break;
-          } else {
-            flg++;
-          }
-        }
-        if ((n2 - nc2) * s2 >= QP_EW_LIMIT) return -2;
-      }
-      if (dir == 0) break;
-      if (flg == 0) {
-        bool stop = qp_comp(dS[2], od2, eps);
-        if (MODE == QP_BOTH) stop = stop && qp_comp(S, oS, eps);
-        if (stop) break;
+  const cplx E2 = expi(L.g2x * r[0] + L.g2y * r[1]);  // phase step along n2
+  int cc = 0, dir = 0, n1 = nc, side = -1, off = 0, flg = 0;
+  int nc2;
+  if (FD) nc2 = (int)round((L.vkx * L.g2x + L.vky * L.g2y - (double)n1 * L.g12) / L.g22);
+  else nc2 = (int)round(-((-L.vkx + (double)n1 * L.g1x) * L.g2x + (-L.vky + (double)n1 * L.g1y) * L.g2y) / L.g22);
+  cplx ph0 = expi((-L.vkx + (double)n1 * L.g1x + (double)nc2 * L.g2x) * r[0] +
+                  (-L.vky + (double)n1 * L.g1y + (double)nc2 * L.g2y) * r[1]);
+  cplx ph = ph0;
+  for (;;) {
+    const int n2 = nc2 + (side == 1 ? -off : off);
+    cplx F, dF[3];
+    int e = FD ? qp_fd_term(L, r, n1, n2, ph, F, dF) : qp_ew2_term(L, r, veps, n1, n2, ph, F, dF);
+    if (!FD) cc++;
+    if (e < 0) return e;
+    S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
+    if (FD) cc++;
+    if (side < 0) {
+      side = 0; off = 1; ph = ph0 * E2;
+      continue;
+    }
+    bool stop = false;
+    if (e > 0) {
+      stop = qp_diff(dF[2], dS[2], eps);
+      if (MODE == QP_BOTH) stop = stop && qp_diff(F, S, eps);
+    } else {
+      flg++;
+    }
+    if (!stop) {
+      if (off + 1 >= LIMIT) return ELIM;
+      off++;
+      ph = ph * (side == 0 ? E2 : conj(E2));
+      continue;
+    }
+    if (side == 0) {
+      side = 1; off = 1; ph = ph0 * conj(E2);
+      continue;
+    }
+    // row finished
+    bool rstop = true;
+    if (dir != 0) {
+      rstop = false;
+      if (FD || flg == 0) {
+        rstop = qp_comp(dS[2], od2, eps);
+        if (MODE == QP_BOTH) rstop = rstop && qp_comp(S, oS, eps);
       }
     }
-    if (dir != 0 && (n1 - nc) * step >= QP_EW_LIMIT) return -2;
-  }
-  const double aidd = fabs(L.idd);
-  S = mul_i(S * (0.25 * aidd));
-  dS[0] = dS[0] * (-0.25 * aidd);
-  dS[1] = dS[1] * (-0.25 * aidd);
-  dS[2] = dS[2] * (0.25 * aidd);
-  return cc;
-}
-
-// Fourier-domain sum (d3_qpgf_d2.c:745-854).  Returns the number of terms or -1/-2/-4.
-template <int MODE>
-BEM_HD int qp_fd_sum(const QPLattice& L, const double* r, double eps, cplx& S, cplx* dS)
-{
-  if (r[2] == 0.0) return -4;
-  int cc = 0;
-  S = mk(0, 0); dS[0] = mk(0, 0); dS[1] = mk(0, 0); dS[2] = mk(0, 0);
-  cplx F, dF[3];
-  const int nc = L.nc1;
-  for (int dir = 0; dir < 3; dir++) {
-    int n1start = (dir == 0) ? nc : (dir == 1 ? nc + 1 : nc - 1);
-    int step = (dir == 2) ? -1 : 1;
-    int n1;
-    for (n1 = n1start; (dir == 0) ? (n1 == nc) : ((n1 - nc) * step < QP_FD_LIMIT); n1 += step) {
-      cplx oS = S, od2 = dS[2];
-      int nc2 = (int)round((L.vkx * L.g2x + L.vky * L.g2y - (double)n1 * L.g12) / L.g22);
-      int e = qp_fd_term(L, r, n1, nc2, F, dF);
-      if (e < 0) return e;
-      S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
-      cc++;
-      for (int side = 0; side < 2; side++) {
-        int s2 = side ? -1 : 1;
-        int n2;
-        for (n2 = nc2 + s2; (n2 - nc2) * s2 < QP_FD_LIMIT; n2 += s2) {
-          e = qp_fd_term(L, r, n1, n2, F, dF);
-          if (e < 0) return e;
-          S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
-          cc++;
-          if (e > 0) {
-            bool stop = qp_diff(dF[2], dS[2], eps);
-            if (MODE == QP_BOTH) stop = stop && qp_diff(F, S, eps);
-            if (stop) break;
-          }
-        }
-        if ((n2 - nc2) * s2 >= QP_FD_LIMIT) return -1;
-      }
-      if (dir == 0) break;
-      bool stop = qp_comp(dS[2], od2, eps);
-      if (MODE == QP_BOTH) stop = stop && qp_comp(S, oS, eps);
-      if (stop) break;
+    if (rstop) {
+      if (dir == 2) break;
+      dir++;
+      n1 = (dir == 1) ? nc + 1 : nc - 1;
+    } else {
+      n1 += (dir == 1) ? 1 : -1;
+      if (n1 - nc >= LIMIT || n1 - nc <= -LIMIT) return ELIM;
     }
-    if (dir != 0 && (n1 - nc) * step >= QP_FD_LIMIT) return -1;
+    oS = S; od2 = dS[2];
+    flg = 0;
+    if (FD) nc2 = (int)round((L.vkx * L.g2x + L.vky * L.g2y - (double)n1 * L.g12) / L.g22);
+    else nc2 = (int)round(-((-L.vkx + (double)n1 * L.g1x) * L.g2x + (-L.vky + (double)n1 * L.g1y) * L.g2y) / L.g22);
+    ph0 = expi((-L.vkx + (double)n1 * L.g1x + (double)nc2 * L.g2x) * r[0] +
+               (-L.vky + (double)n1 * L.g1y + (double)nc2 * L.g2y) * r[1]);
+    ph = ph0;
+    side = -1;
+    off = 0;
   }
   const double aidd = fabs(L.idd);
-  S = mul_i(S * (0.5 * aidd));
-  dS[0] = dS[0] * (-0.5 * aidd);
-  dS[1] = dS[1] * (-0.5 * aidd);
-  dS[2] = dS[2] * (-0.5 * aidd * r[2] / fabs(r[2]));
+  if (FD) {
+    S = mul_i(S * (0.5 * aidd));
+    dS[0] = dS[0] * (-0.5 * aidd);
+    dS[1] = dS[1] * (-0.5 * aidd);
+    dS[2] = dS[2] * (-0.5 * aidd * r[2] / fabs(r[2]));
+  } else {
+    S = mul_i(S * (0.25 * aidd));
+    dS[0] = dS[0] * (-0.25 * aidd);
+    dS[1] = dS[1] * (-0.25 * aidd);
+    dS[2] = dS[2] * (0.25 * aidd);
+  }
   return cc;
 }
 
@@ -346,7 +354,7 @@ BEM_HD int qpgf_eval(const QPLattice& L, const double* r_in, QPVal& out)
   }
   int err;
   if (use_fd) {
-    err = qp_fd_sum<MODE>(L, r, eps, out.G, out.dG);
+    err = qp_spec_sum<MODE, 1>(L, r, 0.0, eps, out.G, out.dG);
     if (err < 0) return err - 10;
   } else {
     // split parameter (d3_qpgf_d2.c:1683-1693)
@@ -357,7 +365,7 @@ BEM_HD int qpgf_eval(const QPLattice& L, const double* r_in, QPVal& out)
     cplx S2, dS2[3];
     int c1 = qp_ew1_sum<MODE>(L, r, veps, eps, out.G, out.dG);
     if (c1 < 0) return c1 - 20;
-    int c2 = qp_ew2_sum<MODE>(L, r, veps, eps, S2, dS2);
+    int c2 = qp_spec_sum<MODE, 0>(L, r, veps, eps, S2, dS2);
     if (c2 < 0) return c2 - 20;
     out.G += S2; out.dG[0] += dS2[0]; out.dG[1] += dS2[1]; out.dG[2] += dS2[2];
     err = c1 + c2;
@@ -423,5 +431,6 @@ BEM_HD int qp_lattice_init(QPLattice& L, double k, double vkx, double vky, doubl
     L.bNm = sqrt(-bNm);
   }
   L.nc1 = n1;
+  L.eb2 = expi(vkx * d2x + vky * d2y);
   return 0;
 }

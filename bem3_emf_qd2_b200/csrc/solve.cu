@@ -144,3 +144,319 @@ __global__ void k_store_bv(SolveDev S, int d, const double* __restrict__ X)
   if (mdid == 0) dphi -= sigm * (tUi[0] * n[0] + tUi[1] * n[1] + tUi[2] * n[2]);
   stc(dU, 3, dphi);
 }
+
+// inv_matrix_33 (:639-660): rows of the inverse of [vn; vtz; vte] as the reference lays them out
+__device__ __forceinline__ void inv33(const double* vn, const double* vtz, const double* vte, double* ma)
+{
+  double i_det = 1.0 / (vn[0] * vtz[1] * vte[2] + vn[1] * vtz[2] * vte[0] + vn[2] * vtz[0] * vte[1] -
+                        (vn[2] * vtz[1] * vte[0] + vn[1] * vtz[0] * vte[2] + vn[0] * vtz[2] * vte[1]));
+  ma[0] = vtz[1] * vte[2] - vtz[2] * vte[1];
+  ma[1] = -vn[1] * vte[2] + vn[2] * vte[1];
+  ma[2] = vn[1] * vtz[2] - vn[2] * vtz[1];
+  ma[3] = -vtz[0] * vte[2] + vtz[2] * vte[0];
+  ma[4] = vn[0] * vte[2] - vn[2] * vte[0];
+  ma[5] = -vn[0] * vtz[2] + vn[2] * vtz[0];
+  ma[6] = vtz[0] * vte[1] - vtz[1] * vte[0];
+  ma[7] = -vn[0] * vte[1] + vn[1] * vte[0];
+  ma[8] = vn[0] * vtz[1] - vn[1] * vtz[0];
+  for (int i = 0; i < 9; i++) ma[i] *= i_det;
+}
+
+// q1_solve_eh_bv (:931-1030) for interior domain d: one warp per collocation node (t, tn).
+// dudt_fcm (:617-637) is the two row dot products over the domain's tangential-derivative rows.
+__global__ void k_eh_interior(SolveDev S, int d)
+{
+  const int ne = S.ne[d];
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= 4 * ne) return;
+  const int t = w >> 2, tn = w & 3;
+  const int at = S.sid_h[d][t], atd = abs(at);
+  Elem el;
+  load_elem(S.geo, atd, el);
+  if (tn == 3 && el.nn == 3) return;
+  const size_t N = (size_t)4 * ne;
+  const double* rz = S.dG[d] + 2 * ((size_t)(2 * (4 * t + tn) + 0) * N);
+  const double* re = S.dG[d] + 2 * ((size_t)(2 * (4 * t + tn) + 1) * N);
+  const double* hz = S.dH[d] + 2 * ((size_t)(2 * (4 * t + tn) + 0) * N);
+  const double* he = S.dH[d] + 2 * ((size_t)(2 * (4 * t + tn) + 1) * N);
+  const double* U = S.U[d];
+  const double* dU = S.dU[d];
+  cplx dUz[4], dUe[4];
+  for (int i = 0; i < 4; i++) { dUz[i] = mk(0, 0); dUe[i] = mk(0, 0); }
+  for (int c = lane; c < 4 * ne; c += 32) {
+    const int s = c >> 2, sn = c & 3;
+    cplx gz = ldc(rz, c), ge = ldc(re, c), hzz = ldc(hz, c), hee = ldc(he, c);
+    const size_t b = (size_t)(4 * (s + 1) + sn) * 4;
+    for (int i = 0; i < 4; i++) {
+      cplx du = ldc(dU, b + i), u = ldc(U, b + i);
+      dUz[i] += gz * du - hzz * u;
+      dUe[i] += ge * du - hee * u;
+    }
+  }
+  for (int i = 0; i < 4; i++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      dUz[i].re += __shfl_xor_sync(0xffffffffu, dUz[i].re, o);
+      dUz[i].im += __shfl_xor_sync(0xffffffffu, dUz[i].im, o);
+      dUe[i].re += __shfl_xor_sync(0xffffffffu, dUe[i].re, o);
+      dUe[i].im += __shfl_xor_sync(0xffffffffu, dUe[i].im, o);
+    }
+  }
+  if (lane != 0) return;
+  const double* tdF = S.dF[d] + 3 * (size_t)(4 * t + tn);
+  const size_t me = (size_t)(4 * (t + 1) + tn) * 4;
+  for (int i = 0; i < 4; i++) {
+    cplx u = ldc(U, me + i);
+    dUz[i] = (dUz[i] - u * tdF[1]) * (1.0 / tdF[0]);
+    dUe[i] = (dUe[i] - u * tdF[2]) * (1.0 / tdF[0]);
+  }
+  double vtz[3], vte[3], vn[3], a[9];
+  node_tangents(el, tn, vtz, vte);
+  const double sig = at < 0 ? -1.0 : 1.0;
+  const double* wn = S.geo + (size_t)atd * GEO_STRIDE + GEO_WEN + 3 * tn;
+  for (int i = 0; i < 3; i++) vn[i] = sig * wn[i];
+  unit3(vn);
+  inv33(vn, vtz, vte, a);
+  const cplx ch = mk(S.ch_re, S.ch_im);
+  cplx dUt[4], Ut[4];
+  for (int i = 0; i < 4; i++) { dUt[i] = ldc(dU, me + i); Ut[i] = ldc(U, me + i); }
+  const size_t me3 = (size_t)(4 * (t + 1) + tn) * 3;
+  for (int i = 0; i < 3; i++)
+    stc(S.E[d], me3 + i, -(dUt[3] * a[i * 3 + 0] + dUz[3] * a[i * 3 + 1] + dUe[3] * a[i * 3 + 2]) + Ut[i]);
+  // H = ch * curl of the potential, written with the rows of a (:987-992)
+  cplx Hv[3];
+  Hv[0] = ch * ((dUt[2] * a[3] + dUz[2] * a[4] + dUe[2] * a[5]) - (dUt[1] * a[6] + dUz[1] * a[7] + dUe[1] * a[8]));
+  Hv[1] = ch * ((dUt[0] * a[6] + dUz[0] * a[7] + dUe[0] * a[8]) - (dUt[2] * a[0] + dUz[2] * a[1] + dUe[2] * a[2]));
+  Hv[2] = ch * ((dUt[1] * a[0] + dUz[1] * a[1] + dUe[1] * a[2]) - (dUt[0] * a[3] + dUz[0] * a[4] + dUe[0] * a[5]));
+  for (int i = 0; i < 3; i++) stc(S.H_[d], me3 + i, Hv[i]);
+  // open-region side of the same node (scattered field, :995-1020)
+  if (S.md[atd] == 0) {
+    const int s0 = S.pos0[atd];
+    const size_t o4 = (size_t)(4 * (s0 + 1) + tn) * 4, o3 = (size_t)(4 * (s0 + 1) + tn) * 3;
+    const double* pz = S.dEiz + 2 * ((size_t)(4 * atd + tn) * 3);
+    const double* pe = S.dEie + 2 * ((size_t)(4 * atd + tn) * 3);
+    cplx dU0[4], U0[4], gz[3], ge[3];
+    for (int i = 0; i < 4; i++) { dU0[i] = ldc(S.dU[0], o4 + i); U0[i] = ldc(S.U[0], o4 + i); }
+    for (int i = 0; i < 3; i++) { gz[i] = dUz[i] - ldc(pz, i); ge[i] = dUe[i] - ldc(pe, i); }
+    for (int i = 0; i < 3; i++)
+      stc(S.E[0], o3 + i, -(-dU0[3] * a[i * 3 + 0] + dUz[3] * a[i * 3 + 1] + dUe[3] * a[i * 3 + 2]) + U0[i]);
+    cplx H0[3];
+    H0[0] = ch * ((-dU0[2] * a[3] + gz[2] * a[4] + ge[2] * a[5]) - (-dU0[1] * a[6] + gz[1] * a[7] + ge[1] * a[8]));
+    H0[1] = ch * ((-dU0[0] * a[6] + gz[0] * a[7] + ge[0] * a[8]) - (-dU0[2] * a[0] + gz[2] * a[1] + ge[2] * a[2]));
+    H0[2] = ch * ((-dU0[1] * a[0] + gz[1] * a[1] + ge[1] * a[2]) - (-dU0[0] * a[3] + gz[0] * a[4] + ge[0] * a[5]));
+    for (int i = 0; i < 3; i++) stc(S.H_[0], o3 + i, H0[i]);
+  }
+}
+
+// solve_deh_bv (:662-791), system of domain d: rows and columns run over the domain's element
+// nodes in order (triangle node 3 skipped).  cmap[c] = 4 s + sn for compacted index c.
+// A row-major (transposed for the column-major solver), B column-major [6][nn].
+__global__ void k_deh_system(SolveDev S, int d, const int* __restrict__ cmap, int nn, double* A, double* B)
+{
+  const int c = blockIdx.x;  // compacted row
+  const int src = cmap[c];   // 4 t + tn
+  const int ne = S.ne[d];
+  const size_t N = (size_t)4 * ne;
+  const double* G = S.G[d] + 2 * ((size_t)src * N);
+  const double* H = S.H[d] + 2 * ((size_t)src * N);
+  double* Ar = A + 2 * (size_t)c * nn;
+  cplx acc[6];
+  for (int j = 0; j < 6; j++) acc[j] = mk(0, 0);
+  for (int r = threadIdx.x; r < nn; r += blockDim.x) {
+    const int col = cmap[r];
+    stc(Ar, r, ldc(G, col));
+    const int s = col >> 2, sn = col & 3;
+    cplx h = ldc(H, col);
+    const size_t b3 = (size_t)(4 * (s + 1) + sn) * 3;
+    for (int i = 0; i < 3; i++) {
+      acc[i] += h * ldc(S.E[d], b3 + i);
+      acc[3 + i] += h * ldc(S.H_[d], b3 + i);
+    }
+  }
+  __shared__ double red[12][256];
+  for (int j = 0; j < 6; j++) { red[2 * j][threadIdx.x] = acc[j].re; red[2 * j + 1][threadIdx.x] = acc[j].im; }
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int j = 0; j < 12; j++) red[j][threadIdx.x] += red[j][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int j = 0; j < 6; j++) stc(B, (size_t)j * nn + c, mk(red[2 * j][0], red[2 * j + 1][0]));
+}
+
+__global__ void k_deh_store(SolveDev S, int d, const int* __restrict__ cmap, int nn, const double* X)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nn) return;
+  const int col = cmap[c];
+  const int s = col >> 2, sn = col & 3;
+  const size_t b3 = (size_t)(4 * (s + 1) + sn) * 3;
+  for (int i = 0; i < 3; i++) {
+    stc(S.dE[d], b3 + i, ldc(X, (size_t)i * nn + c));
+    stc(S.dH_[d], b3 + i, ldc(X, (size_t)(3 + i) * nn + c));
+  }
+}
+
+// ==========================================================================================
+// Host orchestration of the solve stage
+#include <vector>
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+  int alloc(size_t bytes) { return cudaMalloc(&p, bytes) == cudaSuccess ? 0 : BEM3_ERR_CUDA; }
+  template <class T> T* as() { return (T*)p; }
+};
+
+template <class T>
+int upload(DevBuf& b, const T* src, size_t n)
+{
+  if (b.alloc(n * sizeof(T) + 16)) return BEM3_ERR_CUDA;
+  return cudaMemcpy(b.p, src, n * sizeof(T), cudaMemcpyHostToDevice) == cudaSuccess ? 0 : BEM3_ERR_CUDA;
+}
+
+// Dense LU solve of A x = B on the device for row-major A (n x n) and column-major B (n x nrhs):
+// the solver sees A^T (column-major), so the transposed solve gives A x = B.
+int lu_solve_rowmajor(cusolverDnHandle_t h, double* A, int n, double* B, int nrhs)
+{
+  int lwork = 0;
+  if (cusolverDnZgetrf_bufferSize(h, n, n, (cuDoubleComplex*)A, n, &lwork) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_SOLVE;
+  DevBuf work, ipiv, info;
+  if (work.alloc(sizeof(cuDoubleComplex) * (size_t)(lwork > 0 ? lwork : 1)) || ipiv.alloc(sizeof(int) * (size_t)n) ||
+      info.alloc(sizeof(int)))
+    return BEM3_ERR_CUDA;
+  if (cusolverDnZgetrf(h, n, n, (cuDoubleComplex*)A, n, work.as<cuDoubleComplex>(), ipiv.as<int>(), info.as<int>()) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return BEM3_ERR_SOLVE;
+  int hinfo = 0;
+  cudaMemcpy(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost);
+  if (hinfo != 0) return BEM3_ERR_SOLVE;
+  if (cusolverDnZgetrs(h, CUBLAS_OP_T, n, nrhs, (const cuDoubleComplex*)A, n, ipiv.as<int>(), (cuDoubleComplex*)B, n,
+                       info.as<int>()) != CUSOLVER_STATUS_SUCCESS)
+    return BEM3_ERR_SOLVE;
+  cudaMemcpy(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost);
+  return hinfo == 0 ? 0 : BEM3_ERR_SOLVE;
+}
+
+}  // namespace
+
+extern "C" int bem3_solve_bieq_arrays(const bem3_problem* P, bem3_bv* out)
+{
+  if (!P || !out || P->MN < 0 || P->MN + 1 > BEM3_MAXDOM || P->Ne <= 0 || P->NN <= 0) return BEM3_ERR_ARG;
+  const int MN = P->MN, Ne = P->Ne, NN = P->NN;
+  int rc;
+  // ---- inputs to the device
+  std::vector<double> geo((size_t)(Ne + 1) * GEO_STRIDE);
+  if ((rc = bem3_pack_geometry(&P->mesh, geo.data()))) return rc;
+  DevBuf dgeo, dmd, dsd, deni, dkn, dUi, ddUi, dEiz, dEie, dpos0;
+  DevBuf dsid[BEM3_MAXDOM], dGm[BEM3_MAXDOM], dHm[BEM3_MAXDOM], ddG[BEM3_MAXDOM], ddH[BEM3_MAXDOM], ddF[BEM3_MAXDOM];
+  DevBuf bU[BEM3_MAXDOM], bdU[BEM3_MAXDOM], bE[BEM3_MAXDOM], bH[BEM3_MAXDOM], bdE[BEM3_MAXDOM], bdH[BEM3_MAXDOM];
+  if ((rc = upload(dgeo, geo.data(), geo.size())) || (rc = upload(dmd, P->md, (size_t)Ne + 1)) ||
+      (rc = upload(dsd, P->sd, (size_t)Ne + 1)) || (rc = upload(deni, P->eni, (size_t)(Ne + 1) * 4)) ||
+      (rc = upload(dkn, P->kn, (size_t)2 * (MN + 1))) || (rc = upload(dUi, P->Ui, (size_t)(Ne + 1) * 32)) ||
+      (rc = upload(ddUi, P->dUi, (size_t)(Ne + 1) * 32)) || (rc = upload(dEiz, P->dEiz, (size_t)(Ne + 1) * 24)) ||
+      (rc = upload(dEie, P->dEie, (size_t)(Ne + 1) * 24)))
+    return rc;
+  std::vector<int> pos0((size_t)Ne + 1, -1);
+  for (int s = 0; s < P->Ne_d[0]; s++) {
+    int a = P->sid[0][s];
+    if (a > 0 && a <= Ne) pos0[a] = s;
+  }
+  if ((rc = upload(dpos0, pos0.data(), pos0.size()))) return rc;
+
+  SolveDev S;
+  memset(&S, 0, sizeof S);
+  S.MN = MN; S.NN = NN; S.Ne = Ne;
+  S.geo = dgeo.as<double>(); S.md = dmd.as<int>(); S.sd = dsd.as<int>(); S.eni = deni.as<int>();
+  S.kn = dkn.as<double>(); S.Ui = dUi.as<double>(); S.dUi = ddUi.as<double>();
+  S.dEiz = dEiz.as<double>(); S.dEie = dEie.as<double>(); S.pos0 = dpos0.as<int>();
+  const double two_pi = 2.0 * QP_PI;
+  S.ch_re = 0.0; S.ch_im = -P->lambda0 / two_pi;  // lambda0 / (2 pi i)
+
+  // ---- assembly of every domain (kept resident for the solve)
+  for (int d = 0; d <= MN; d++) {
+    const int ne = P->Ne_d[d];
+    const size_t N = (size_t)4 * ne;
+    S.ne[d] = ne;
+    if ((rc = upload(dsid[d], P->sid[d], (size_t)ne))) return rc;
+    if (dGm[d].alloc(N * N * 16) || dHm[d].alloc(N * N * 16) || ddG[d].alloc(2 * N * N * 16) ||
+        ddH[d].alloc(2 * N * N * 16) || ddF[d].alloc(N * 3 * 8))
+      return BEM3_ERR_CUDA;
+    int periodic = (d == 0 && P->ps == 1) ? 1 : 0;
+    rc = bem3_assemble_domain_dev(dgeo.as<double>(), Ne, dsid[d].as<int>(), ne, d, periodic, &P->qd, P->kn[2 * d],
+                                  P->kn[2 * d + 1], dGm[d].as<double>(), dHm[d].as<double>(), ddG[d].as<double>(),
+                                  ddH[d].as<double>(), ddF[d].as<double>(), nullptr);
+    if (rc) return rc;
+    S.sid_h[d] = dsid[d].as<int>();
+    S.G[d] = dGm[d].as<double>(); S.H[d] = dHm[d].as<double>();
+    S.dG[d] = ddG[d].as<double>(); S.dH[d] = ddH[d].as<double>(); S.dF[d] = ddF[d].as<double>();
+    const size_t nb4 = (size_t)(ne + 1) * 4 * 4 * 16, nb3 = (size_t)(ne + 1) * 4 * 3 * 16;
+    if (bU[d].alloc(nb4) || bdU[d].alloc(nb4) || bE[d].alloc(nb3) || bH[d].alloc(nb3) || bdE[d].alloc(nb3) ||
+        bdH[d].alloc(nb3))
+      return BEM3_ERR_CUDA;
+    cudaMemset(bU[d].p, 0, nb4); cudaMemset(bdU[d].p, 0, nb4);
+    cudaMemset(bE[d].p, 0, nb3); cudaMemset(bH[d].p, 0, nb3); cudaMemset(bdE[d].p, 0, nb3); cudaMemset(bdH[d].p, 0, nb3);
+    S.U[d] = bU[d].as<double>(); S.dU[d] = bdU[d].as<double>(); S.E[d] = bE[d].as<double>();
+    S.H_[d] = bH[d].as<double>(); S.dE[d] = bdE[d].as<double>(); S.dH_[d] = bdH[d].as<double>();
+  }
+
+  // ---- global system (create_tmatrix_csr row order) and its LU solve
+  std::vector<int4> rowmap;
+  rowmap.reserve((size_t)8 * NN);
+  for (int d = 0; d <= MN; d++)
+    for (int cid = 0; cid < 4; cid++)
+      for (int t = 0; t < P->Ne_d[d]; t++) {
+        int a = abs(P->sid[d][t]);
+        int nv = P->mesh.nv[a];
+        for (int tn = 0; tn < nv; tn++) rowmap.push_back(make_int4(d, cid, t, tn));
+      }
+  const long long na = (long long)8 * NN;
+  if ((long long)rowmap.size() != na) return BEM3_ERR_ARG;
+  DevBuf drow, dA, dB;
+  if ((rc = upload(drow, rowmap.data(), rowmap.size()))) return rc;
+  if (dA.alloc((size_t)na * na * 16) || dB.alloc((size_t)na * 16)) return BEM3_ERR_CUDA;
+  cudaMemset(dA.p, 0, (size_t)na * na * 16);
+  k_build_rows<<<(unsigned)na, 256>>>(S, drow.as<int4>(), dA.as<double>(), dB.as<double>(), na);
+  if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
+  cusolverDnHandle_t h = nullptr;
+  if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
+  rc = lu_solve_rowmajor(h, dA.as<double>(), (int)na, dB.as<double>(), 1);
+  if (rc) { cusolverDnDestroy(h); return rc; }
+  for (int d = 0; d <= MN; d++) k_store_bv<<<(4 * S.ne[d] + 127) / 128, 128>>>(S, d, dB.as<double>());
+  // ---- boundary fields E, H (interior domains, and the open-region side of their nodes)
+  for (int d = 1; d <= MN; d++) k_eh_interior<<<(4 * S.ne[d] * 32 + 255) / 256, 256>>>(S, d);
+  // ---- normal derivatives dE, dH per domain
+  for (int d = 0; d <= MN && rc == 0; d++) {
+    std::vector<int> cmap;
+    for (int t = 0; t < P->Ne_d[d]; t++) {
+      int nv = P->mesh.nv[abs(P->sid[d][t])];
+      for (int tn = 0; tn < nv; tn++) cmap.push_back(4 * t + tn);
+    }
+    const int nn = (int)cmap.size();
+    DevBuf dc, dAd, dBd;
+    if ((rc = upload(dc, cmap.data(), cmap.size()))) break;
+    if (dAd.alloc((size_t)nn * nn * 16) || dBd.alloc((size_t)nn * 6 * 16)) { rc = BEM3_ERR_CUDA; break; }
+    k_deh_system<<<nn, 256>>>(S, d, dc.as<int>(), nn, dAd.as<double>(), dBd.as<double>());
+    rc = lu_solve_rowmajor(h, dAd.as<double>(), nn, dBd.as<double>(), 6);
+    if (rc) break;
+    k_deh_store<<<(nn + 127) / 128, 128>>>(S, d, dc.as<int>(), nn, dBd.as<double>());
+  }
+  cusolverDnDestroy(h);
+  if (rc) return rc;
+  if (cudaDeviceSynchronize() != cudaSuccess) return BEM3_ERR_CUDA;
+  // ---- results back to the caller
+  for (int d = 0; d <= MN; d++) {
+    const int ne = S.ne[d];
+    const size_t nb4 = (size_t)(ne + 1) * 4 * 4 * 16, nb3 = (size_t)(ne + 1) * 4 * 3 * 16;
+    if ((out[d].U && cudaMemcpy(out[d].U, bU[d].p, nb4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (out[d].dU && cudaMemcpy(out[d].dU, bdU[d].p, nb4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (out[d].E && cudaMemcpy(out[d].E, bE[d].p, nb3, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (out[d].H && cudaMemcpy(out[d].H, bH[d].p, nb3, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (out[d].dE && cudaMemcpy(out[d].dE, bdE[d].p, nb3, cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (out[d].dH && cudaMemcpy(out[d].dH, bdH[d].p, nb3, cudaMemcpyDeviceToHost) != cudaSuccess))
+      return BEM3_ERR_CUDA;
+  }
+  return 0;
+}

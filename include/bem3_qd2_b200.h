@@ -111,6 +111,39 @@ int bem3_last_stats(bem3_stats *out);
  * FP64 roofline.  Runs a ~100 ms kernel. */
 double bem3_fp64_peak_tflops(void);
 
+/* ---------------------------------------------------------------------------------------------
+ * Boundary-integral equation solve.
+ * Replaces solve_bieq (d3qd2_src/d3qd2_solve_bieq.c:36-84) on arrays: assembles every domain
+ * (create_cmatrix, :156-256), builds the global system of 8 NN unknowns (create_matrix_csr_dac,
+ * :284-421), solves it with a dense device LU (in place of PARDISO, d3qd2_mkl_solver.c:18),
+ * stores U, dU (tmatrix_bd_store, :456-544), computes E, H on the boundary (q1_solve_eh_bv,
+ * :931-1030) and dE, dH (solve_deh_bv, :662-791).  Everything runs on the current CUDA device;
+ * the dense system needs (8 NN)^2 * 16 bytes of device memory.
+ * Layouts follow DQD2 (d3qd2_src/d3qd2_elem.h:13-60), flattened, element ids 1..Ne (slot 0 unused). */
+typedef struct {
+  int MN;                   /* media 1..MN; domain 0 is the open region */
+  int Ne, NN;               /* elements; element nodes (3 per triangle, 4 per quad) */
+  int ps;                   /* 1: quasi-periodic open region */
+  bem3_mesh mesh;
+  const int *md, *sd;       /* [(Ne+1)] main / sub domain of each element */
+  const int *eni;           /* [(Ne+1)][4] element node ids (-1 for the 4th node of triangles) */
+  const int *Ne_d;          /* [MN+1] elements per domain */
+  const int *const *sid;    /* [MN+1] -> [Ne_d] signed element ids (sb[d].sid[1..Ne_d]) */
+  const double *kn;         /* [MN+1] complex wave numbers */
+  bem3_qpd2 qd;
+  double lambda0;
+  const double *Ui, *dUi;   /* [(Ne+1)][4][4] complex incident potential and normal derivative */
+  const double *dEiz, *dEie;/* [(Ne+1)][4][3] complex tangential derivatives of the incident E */
+} bem3_problem;
+
+/* Boundary values of one domain, same layout as SUBD (d3qd2_elem.h:13-20), slot 0 unused:
+ * U, dU [(Ne_d+1)][4][4], E, dE, H, dH [(Ne_d+1)][4][3] complex.  NULL members are skipped. */
+typedef struct {
+  double *U, *dU, *E, *dE, *H, *dH;
+} bem3_bv;
+
+int bem3_solve_bieq_arrays(const bem3_problem *P, bem3_bv *out /* [MN+1] */);
+
 /* Gauss-Legendre nodes and weights on [-1, 1] (the reference's gauleg, com_src/gauleg.c:3). */
 void bem3_gauss_legendre(int n, double *x, double *w);
 
