@@ -284,3 +284,70 @@ extern "C" double bem3_fp64_peak_tflops(void)
 }
 
 extern "C" const char* bem3_version(void) { return "bem3_emf_qd2_b200 0.1 (sm_100a, FP64)"; }
+
+// ------------------------------------------------------------------------------------------
+// Assembly without device allocation.
+//
+// Some callers cannot call cudaMalloc: a serving process that hands every byte of HBM out of
+// its own pool under a fixed budget (allocations outside the pool are forbidden), or a
+// pipeline that must not hit the implicit device-wide synchronisation cudaMalloc/cudaFree can
+// cause.  For them the per-call scratch of the assembly (the chunk's F row-sum terms, the
+// near-singular work list, the status word) lives in this file-scope device array instead of
+// the cudaMalloc'd pool used by bem3_assemble_domain_dev.  Every GPU that loads the library
+// holds the array (BEM3_NOALLOC_SCRATCH_BYTES) until the process exits.
+#define BEM3_NOALLOC_SCRATCH_BYTES (32u << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[BEM3_NOALLOC_SCRATCH_BYTES];
+static void* g_noalloc_addr[MAX_DEV];  // device address of g_noalloc_scratch, per device
+static std::mutex g_noalloc_mu;
+
+extern "C" int bem3_assemble_domain_dev_noalloc(const double* geo_dev, int Ne, const int* sid_dev, int Ne_d, int did,
+                                                int periodic, const bem3_qpd2* qd, double kre, double kim,
+                                                double* G_dev, double* H_dev, double* dG_dev, double* dH_dev,
+                                                double* dF_dev, void* stream)
+{
+  if (!geo_dev || !sid_dev || Ne <= 0 || Ne_d <= 0 || Ne_d > 2 * Ne || !G_dev || !H_dev) return BEM3_ERR_ARG;
+  QPLattice L;
+  memset(&L, 0, sizeof L);
+  if (periodic) {
+    int e = lattice_from(qd, &L);
+    if (e) return e;
+  }
+  // The array's device address: host code may not use the symbol itself (that is a host-side
+  // stand-in, not a device pointer), so resolve it once per device with that device current.
+  const int dev = cur_dev();
+  if (dev < 0 || dev >= MAX_DEV) return BEM3_ERR_ARG;
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return BEM3_ERR_CUDA;
+      g_noalloc_addr[dev] = p;
+    }
+    base = g_noalloc_addr[dev];
+  }
+  // [0, 256): status word; [256, end): assembly scratch, chunked to fit
+  int* status = (int*)base;
+  void* scratch = (char*)base + 256;
+  const size_t avail = BEM3_NOALLOC_SCRATCH_BYTES - 256;
+  int rows = default_rows_per_chunk(Ne_d);
+  while (rows > 4 && bem3_scratch_bytes(Ne_d, rows) > avail) rows = rows / 2 > 4 ? rows / 2 : 4;
+  if (bem3_scratch_bytes(Ne_d, rows) > avail) return BEM3_ERR_SCRATCH;  // domain too large for the array
+  cudaStream_t st = (cudaStream_t)stream;
+  AssembleArgs A;
+  A.geo = geo_dev; A.sid = sid_dev; A.ne = Ne_d; A.did = did; A.periodic = periodic ? 1 : 0;
+  A.kre = kre; A.kim = kim;
+  A.G = G_dev; A.H = H_dev; A.dG = dG_dev; A.dH = dH_dev; A.dF = dF_dev;
+  A.terms = nullptr;
+  // the array keeps the previous call's contents: the status word must start at zero (the
+  // run itself clears its row-sum slots and work-list counter before use)
+  if (cudaMemsetAsync(status, 0, sizeof(int), st) != cudaSuccess) return BEM3_ERR_CUDA;
+  AssembleStats S;
+  memset(&S, 0, sizeof S);
+  int e = bem3_assemble_run(A, &L, scratch, avail, rows, status, st, &S);
+  if (e) return e;
+  int hs = 0;
+  if (cudaMemcpyAsync(&hs, status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return BEM3_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return BEM3_ERR_CUDA;
+  return hs;
+}

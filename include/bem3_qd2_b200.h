@@ -87,6 +87,20 @@ int bem3_assemble_domain_dev(const double *geo_dev, int Ne, const int *sid_dev, 
                              const bem3_qpd2 *qd, double kre, double kim, double *G_dev, double *H_dev,
                              double *dG_dev, double *dH_dev, double *dF_dev, void *stream);
 
+/* Same as bem3_assemble_domain_dev, for callers that cannot allocate device memory (a serving
+ * process whose pool owns all of HBM under a fixed budget, a pipeline that must avoid the implicit
+ * synchronisation of cudaMalloc/cudaFree).  No counterpart in the reference, whose assembly runs
+ * on the host.  The call allocates nothing: its scratch is a 32 MiB file-scope device array that
+ * every GPU loading the library holds until exit, and regular pairs are processed in row chunks
+ * that fit it.  A domain whose four rows of one element do not fit (about 170,000 elements per
+ * domain) is rejected with BEM3_ERR_SCRATCH.  All calls share the array: calls that overlap on the
+ * GPU (other streams, other threads on the same device) race and must be serialised by the caller.
+ * The first call on a device resolves the array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  Synchronous on `stream`. */
+int bem3_assemble_domain_dev_noalloc(const double *geo_dev, int Ne, const int *sid_dev, int Ne_d, int did, int periodic,
+                                     const bem3_qpd2 *qd, double kre, double kim, double *G_dev, double *H_dev,
+                                     double *dG_dev, double *dH_dev, double *dF_dev, void *stream);
+
 /* Packs a bem3_mesh into the device geometry layout: (Ne+1) * bem3_geo_stride() doubles. */
 int bem3_geo_stride(void);
 int bem3_pack_geometry(const bem3_mesh *mesh, double *geo);

@@ -1,0 +1,104 @@
+"""bem3_assemble_domain_dev_noalloc (scratch in a static device array) against
+bem3_assemble_domain_dev (scratch from cudaMalloc) on the same device inputs.
+
+Two calls in a row per case: the second call finds the static array holding the first call's
+row sums, work list and status, so it checks that everything which must start at zero does.
+Tolerance: |noalloc - dev| <= 1e-12 * max |dev| per matrix (same kernels, same per-row order).
+The twolayer3072 interior domain (3072 elements) does not fit the array in one chunk, so it
+also runs the chunked path that the static size forces.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def _golden_problem(case):
+    from bem3_emf_qd2_b200.dqd2 import problem_from_arrays
+    g = golden(f"rows_{case}.npz")
+    return problem_from_arrays({k[3:]: g[k] for k in g.files if k.startswith("in/")})
+
+
+def _entry(B):
+    L = B.lib()
+    f = L.bem3_assemble_domain_dev_noalloc
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    f.argtypes = [vp, i, vp, i, i, i, C.POINTER(B.bem3_qpd2), d, d, vp, vp, vp, vp, vp, vp]
+    f.restype = i
+    return f
+
+
+def _outputs(torch, ne, dev):
+    n = 4 * ne
+    G = torch.full((n, n), complex(np.nan, np.nan), dtype=torch.complex128, device=dev)
+    return dict(G=G, H=torch.full_like(G, complex(np.nan, np.nan)),
+                dG=torch.full((2 * n, n), complex(np.nan, np.nan), dtype=torch.complex128, device=dev),
+                dH=torch.full((2 * n, n), complex(np.nan, np.nan), dtype=torch.complex128, device=dev),
+                dF=torch.full((n, 3), np.nan, dtype=torch.float64, device=dev))
+
+
+def _run(fn, B, P, dp, did, out):
+    k = complex(P.kn[did])
+    ne = len(P.sid[did])
+    periodic = 1 if (did == 0 and P.ps == 1) else 0
+    rc = fn(dp.geo.data_ptr(), P.Ne, dp.sids[did].data_ptr(), ne, did, periodic, C.byref(dp.q), k.real, k.imag,
+            out["G"].data_ptr(), out["H"].data_ptr(), out["dG"].data_ptr(), out["dH"].data_ptr(),
+            out["dF"].data_ptr(), None)
+    return rc
+
+
+def _check(B, P, did):
+    import torch
+    dev = "cuda:0"
+    dp = B.DeviceProblem(P, device=dev)
+    ne = len(P.sid[did])
+    ref = _outputs(torch, ne, dev)
+    assert _run(B.lib().bem3_assemble_domain_dev, B, P, dp, did, ref) == 0
+    torch.cuda.synchronize()
+    fn = _entry(B)
+    for call in range(2):
+        got = _outputs(torch, ne, dev)
+        rc = _run(fn, B, P, dp, did, got)
+        assert rc == 0, (did, call, rc)
+        torch.cuda.synchronize()
+        for name in ("G", "H", "dG", "dH", "dF"):
+            r, g = ref[name], got[name]
+            assert bool(torch.isfinite(r).all()), name
+            scale = float(r.abs().max())
+            err = float((g - r).abs().max())
+            assert err <= TOL * max(scale, 1e-300), (did, call, name, err, scale)
+        del got
+    del ref, dp
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("case,did", [("sphere_m4", 0), ("sphere_m4", 1), ("cone_m1", 0), ("cone_m1", 1)])
+def test_noalloc_matches_allocating_entry(cuda_lib, case, did):
+    _check(cuda_lib, _golden_problem(case), did)
+
+
+def test_noalloc_chunked_interior(cuda_lib, tmp_path):
+    from bem3_emf_qd2_b200 import meshgen
+    P, _ = meshgen.problem("twolayer3072", str(tmp_path))
+    assert len(P.sid[1]) == 3072
+    _check(cuda_lib, P, 1)
+
+
+def test_noalloc_rejects_bad_arguments_and_oversized_domains(cuda_lib):
+    import torch
+    fn = _entry(cuda_lib)
+    q = cuda_lib.bem3_qpd2()
+    BEM3_ERR_ARG, BEM3_ERR_SCRATCH = -1, -3
+    assert fn(None, 1, None, 1, 0, 0, C.byref(q), 1.0, 0.0, None, None, None, None, None, None) == BEM3_ERR_ARG
+    # 200,000 elements in one domain: the row-sum slots alone exceed the static array, so the
+    # call is refused before any kernel reads the (placeholder) buffers.
+    dummy = torch.zeros(16, dtype=torch.float64, device="cuda:0")
+    p = dummy.data_ptr()
+    rc = fn(p, 100000, p, 200000, 1, 0, C.byref(q), 1.0, 0.0, p, p, p, p, p, None)
+    assert rc == BEM3_ERR_SCRATCH
