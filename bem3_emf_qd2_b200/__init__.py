@@ -51,14 +51,33 @@ class bem3_qpd2(C.Structure):
     _fields_ = [("k", C.c_double), ("vk", C.c_double * 3), ("vd1", C.c_double * 2), ("vd2", C.c_double * 2)]
 
 
-class bem3_stats(C.Structure):
-    _fields_ = [("gh_pairs", C.c_ulonglong), ("qpgf_terms", C.c_ulonglong), ("launches", C.c_int),
-                ("reg_periodic_launches", C.c_int), ("reg_periodic_ms", C.c_double)]
-
-
 class bem3_mesh(C.Structure):
     _fields_ = [("Ne", C.c_int), ("cr", C.c_void_p), ("cw", C.c_void_p), ("ren", C.c_void_p),
                 ("wen", C.c_void_p), ("nv", C.c_void_p)]
+
+
+class bem3_wave(C.Structure):
+    _fields_ = [("E0", C.c_double), ("ki", C.c_double), ("cos_t", C.c_double), ("sin_t", C.c_double),
+                ("cos_p", C.c_double), ("sin_p", C.c_double), ("f", C.c_double * 3), ("e", C.c_double * 6),
+                ("h", C.c_double * 6)]
+
+
+class bem3_problem(C.Structure):
+    _fields_ = [("MN", C.c_int), ("Ne", C.c_int), ("NN", C.c_int), ("ps", C.c_int), ("mesh", bem3_mesh),
+                ("md", C.c_void_p), ("sd", C.c_void_p), ("eni", C.c_void_p), ("Ne_d", C.c_void_p),
+                ("sid", C.c_void_p), ("kn", C.c_void_p), ("qd", bem3_qpd2), ("lambda0", C.c_double),
+                ("Ui", C.c_void_p), ("dUi", C.c_void_p), ("dEiz", C.c_void_p), ("dEie", C.c_void_p),
+                ("Nn", C.c_int), ("rn", C.c_void_p), ("ed", C.c_void_p), ("nwaves", C.c_int),
+                ("waves", C.c_void_p)]
+
+
+class bem3_bv(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("U", "dU", "E", "dE", "H", "dH")]
+
+
+class bem3_stats(C.Structure):
+    _fields_ = [("gh_pairs", C.c_ulonglong), ("qpgf_terms", C.c_ulonglong), ("launches", C.c_int),
+                ("reg_periodic_launches", C.c_int), ("reg_periodic_ms", C.c_double)]
 
 
 _lib = None
@@ -78,6 +97,16 @@ def lib():
                                            vp, vp, vp, vp, vp]
         L.bem3_assemble_domain_dev.argtypes = [vp, i, vp, i, i, i, C.POINTER(bem3_qpd2), d, d, vp, vp, vp, vp, vp, vp]
         L.bem3_pack_geometry.argtypes = [C.POINTER(bem3_mesh), vp]
+        L.bem3_solve_bieq_arrays.argtypes = [C.POINTER(bem3_problem), C.POINTER(bem3_bv)]
+        L.bem3_ctx_create.argtypes = [C.POINTER(bem3_problem), C.POINTER(C.c_void_p)]
+        L.bem3_ctx_destroy.argtypes = [vp]
+        L.bem3_ctx_destroy.restype = None
+        L.bem3_ctx_solve.argtypes = [vp]
+        L.bem3_ctx_set_solver.argtypes = [vp, i]
+        L.bem3_ctx_get_bv.argtypes = [vp, C.POINTER(bem3_bv)]
+        L.bem3_ctx_set_bv.argtypes = [vp, C.POINTER(bem3_bv)]
+        L.bem3_ctx_domain_id.argtypes = [vp, i, vp, vp]
+        L.bem3_ctx_field.argtypes = [vp, i, vp, i, i, vp, vp, vp]
         L.bem3_geo_stride.restype = i
         L.bem3_last_gh_pairs.restype = C.c_ulonglong
         L.bem3_gauss_legendre.argtypes = [i, vp, vp]
@@ -156,6 +185,123 @@ def assemble_domain(problem: Problem, did: int, derivatives: bool = True):
                                     _ptr(dH) if dH is not None else None, _ptr(dF))
     check(rc, "bem3_assemble_domain")
     return dict(G=G, H=H, dG=dG, dH=dH, dF=dF, gh_pairs=int(lib().bem3_last_gh_pairs()))
+
+
+class ProblemArrays:
+    """A bem3_problem over arrays kept alive by this object."""
+
+    def __init__(self, problem: Problem):
+        p = problem
+        self.ma = MeshArrays(p)
+        self.md = np.ascontiguousarray(p.md, dtype=np.int32)
+        self.sd = np.ascontiguousarray(p.sd, dtype=np.int32)
+        self.eni = np.ascontiguousarray(p.eni, dtype=np.int32)
+        self.ne_d = np.array([len(s) for s in p.sid], np.int32)
+        self.sids = [np.ascontiguousarray(s, dtype=np.int32) for s in p.sid]
+        self.sid_ptrs = (C.c_void_p * len(self.sids))(*[s.ctypes.data for s in self.sids])
+        self.kn = np.ascontiguousarray(np.array(p.kn, np.complex128))
+        self.Ui = np.ascontiguousarray(p.Ui)
+        self.dUi = np.ascontiguousarray(p.dUi)
+        dEz, dEe = p.incident_tangent_derivatives()
+        self.dEiz = np.ascontiguousarray(dEz)
+        self.dEie = np.ascontiguousarray(dEe)
+        self.rn = np.ascontiguousarray(p.rn, dtype=np.float64)
+        self.ed = np.ascontiguousarray(p.ed, dtype=np.int32)
+        self.waves = (bem3_wave * len(p.waves))()
+        for j, w in enumerate(p.waves):
+            W = self.waves[j]
+            W.E0, W.ki, W.cos_t, W.sin_t, W.cos_p, W.sin_p = w.E0, w.ki, w.cos_t, w.sin_t, w.cos_p, w.sin_p
+            for l in range(3):
+                W.f[l] = w.f[l]
+            for l, (ev, hv) in enumerate(((w.ex, w.hx), (w.ey, w.hy), (w.ez, w.hz))):
+                W.e[2 * l], W.e[2 * l + 1] = complex(ev).real, complex(ev).imag
+                W.h[2 * l], W.h[2 * l + 1] = complex(hv).real, complex(hv).imag
+        self.s = bem3_problem(p.MN, p.Ne, p.NN, p.ps, self.ma.m, _ptr(self.md), _ptr(self.sd), _ptr(self.eni),
+                              _ptr(self.ne_d), C.cast(self.sid_ptrs, C.c_void_p), _ptr(self.kn), make_qpd(p.qpd),
+                              p.lambda0, _ptr(self.Ui), _ptr(self.dUi), _ptr(self.dEiz), _ptr(self.dEie),
+                              self.rn.shape[0] - 1, _ptr(self.rn), _ptr(self.ed), len(p.waves),
+                              C.cast(self.waves, C.c_void_p))
+
+
+def _bv_arrays(problem: Problem):
+    out = []
+    bvs = (bem3_bv * (problem.MN + 1))()
+    for d in range(problem.MN + 1):
+        ne = len(problem.sid[d])
+        r = dict(U=np.zeros((ne + 1, 4, 4), np.complex128), dU=np.zeros((ne + 1, 4, 4), np.complex128))
+        for k in ("E", "dE", "H", "dH"):
+            r[k] = np.zeros((ne + 1, 4, 3), np.complex128)
+        for k, v in r.items():
+            setattr(bvs[d], k, v.ctypes.data)
+        out.append(r)
+    return out, bvs
+
+
+class Context:
+    """A problem resident on the current CUDA device (bem3_ctx): solve, boundary values, fields."""
+
+    def __init__(self, problem: Problem):
+        self.p = problem
+        self.pa = ProblemArrays(problem)
+        self.h = C.c_void_p()
+        check(lib().bem3_ctx_create(C.byref(self.pa.s), C.byref(self.h)), "bem3_ctx_create")
+
+    def close(self) -> None:
+        if self.h:
+            lib().bem3_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, method: int = 0) -> None:
+        """method 0: reduced 4 NN system where applicable, 1: the full 8 NN system, 2: reduced only."""
+        check(lib().bem3_ctx_set_solver(self.h, method), "bem3_ctx_set_solver")
+        check(lib().bem3_ctx_solve(self.h), "bem3_ctx_solve")
+
+    def boundary_values(self):
+        out, bvs = _bv_arrays(self.p)
+        check(lib().bem3_ctx_get_bv(self.h, bvs), "bem3_ctx_get_bv")
+        return out
+
+    def set_boundary_values(self, bv) -> None:
+        keep, bvs = [], (bem3_bv * (self.p.MN + 1))()
+        for d in range(self.p.MN + 1):
+            for k in ("U", "dU", "E", "dE", "H", "dH"):
+                a = np.ascontiguousarray(bv[d][k], dtype=np.complex128)
+                keep.append(a)
+                setattr(bvs[d], k, a.ctypes.data)
+        check(lib().bem3_ctx_set_bv(self.h, bvs), "bem3_ctx_set_bv")
+
+    def domain_id(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+        did = np.zeros(len(r), np.int32)
+        check(lib().bem3_ctx_domain_id(self.h, len(r), _ptr(r), _ptr(did)), "bem3_ctx_domain_id")
+        return did
+
+    def field(self, r, type_: int = 0, total: bool = True):
+        """E, H [n,3] complex and the domain of each point (EH_t if total else EH_s)."""
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+        E = np.zeros((len(r), 3), np.complex128)
+        H = np.zeros((len(r), 3), np.complex128)
+        did = np.zeros(len(r), np.int32)
+        check(lib().bem3_ctx_field(self.h, len(r), _ptr(r), type_, 1 if total else 0, _ptr(E), _ptr(H), _ptr(did)),
+              "bem3_ctx_field")
+        return E, H, did
+
+
+def solve_bieq(problem: Problem):
+    """Boundary values of every domain (solve_bieq, d3qd2_src/d3qd2_solve_bieq.c:36-84) on the GPU.
+
+    Returns a list over domains 0..MN of dicts U, dU [(Ne_d+1),4,4] and E, H, dE, dH
+    [(Ne_d+1),4,3] (complex, slot 0 unused), the arrays SUBD holds (d3qd2_elem.h:13-20)."""
+    pa = ProblemArrays(problem)
+    out, bvs = _bv_arrays(problem)
+    check(lib().bem3_solve_bieq_arrays(C.byref(pa.s), bvs), "bem3_solve_bieq_arrays")
+    return out
 
 
 def gauss_legendre(n: int):

@@ -4,3 +4,6 @@
 #include "self_interior.cu"
 #include "capi.cu"
 #include "solve.cu"
+#include "field.cu"
+#include "solve_dtn.cu"
+#include "context.cu"

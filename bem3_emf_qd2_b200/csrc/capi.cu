@@ -20,6 +20,7 @@ struct DevRes {
   size_t scratch_bytes = 0;
   int* status = nullptr;  // device int
   unsigned long long* terms = nullptr;  // device counter (profiling only)
+  QPProp* prop = nullptr;               // propagating orders of the lattice being assembled
 };
 
 std::mutex g_mu;
@@ -51,6 +52,19 @@ int ensure_scratch(size_t bytes, DevRes** out)
     r.scratch_bytes = bytes;
   }
   *out = &r;
+  return 0;
+}
+
+// The lattice's propagating orders into device memory `dst` (QP_PROP_CAP entries) on `st`, for
+// the hoisted spectral sums; without room the sums keep the reference's order (nprop = -1).
+int attach_prop_list(QPLattice* L, QPProp* dst, cudaStream_t st)
+{
+  static thread_local QPProp host[QP_PROP_CAP];
+  const int n = qp_prop_list(*L, host, QP_PROP_CAP);
+  L->prop = dst;
+  L->nprop = n;
+  if (n > 0 && cudaMemcpyAsync(dst, host, sizeof(QPProp) * (size_t)n, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return BEM3_ERR_CUDA;
   return 0;
 }
 
@@ -177,6 +191,10 @@ extern "C" int bem3_assemble_domain_dev(const double* geo_dev, int Ne, const int
   A.geo = geo_dev; A.sid = sid_dev; A.ne = Ne_d; A.did = did; A.periodic = periodic ? 1 : 0;
   A.kre = kre; A.kim = kim;
   A.G = G_dev; A.H = H_dev; A.dG = dG_dev; A.dH = dH_dev; A.dF = dF_dev;
+  if (periodic) {
+    if (!R->prop && cudaMalloc(&R->prop, sizeof(QPProp) * QP_PROP_CAP) != cudaSuccess) return BEM3_ERR_CUDA;
+    if ((e = attach_prop_list(&L, R->prop, st))) return e;
+  }
   if (cudaMemsetAsync(R->status, 0, sizeof(int), st) != cudaSuccess) return BEM3_ERR_CUDA;
   A.terms = nullptr;
   if (t_profiling) {
@@ -326,10 +344,13 @@ extern "C" int bem3_assemble_domain_dev_noalloc(const double* geo_dev, int Ne, c
     }
     base = g_noalloc_addr[dev];
   }
-  // [0, 256): status word; [256, end): assembly scratch, chunked to fit
+  // [0, 256): status word; then the lattice's propagating orders; then the assembly scratch,
+  // chunked to fit
   int* status = (int*)base;
-  void* scratch = (char*)base + 256;
-  const size_t avail = BEM3_NOALLOC_SCRATCH_BYTES - 256;
+  QPProp* prop = (QPProp*)((char*)base + 256);
+  const size_t head = 256 + sizeof(QPProp) * QP_PROP_CAP;
+  void* scratch = (char*)base + head;
+  const size_t avail = BEM3_NOALLOC_SCRATCH_BYTES - head;
   int rows = default_rows_per_chunk(Ne_d);
   while (rows > 4 && bem3_scratch_bytes(Ne_d, rows) > avail) rows = rows / 2 > 4 ? rows / 2 : 4;
   if (bem3_scratch_bytes(Ne_d, rows) > avail) return BEM3_ERR_SCRATCH;  // domain too large for the array
@@ -339,6 +360,10 @@ extern "C" int bem3_assemble_domain_dev_noalloc(const double* geo_dev, int Ne, c
   A.kre = kre; A.kim = kim;
   A.G = G_dev; A.H = H_dev; A.dG = dG_dev; A.dH = dH_dev; A.dF = dF_dev;
   A.terms = nullptr;
+  if (periodic) {
+    int e2 = attach_prop_list(&L, prop, st);
+    if (e2) return e2;
+  }
   // the array keeps the previous call's contents: the status word must start at zero (the
   // run itself clears its row-sum slots and work-list counter before use)
   if (cudaMemsetAsync(status, 0, sizeof(int), st) != cudaSuccess) return BEM3_ERR_CUDA;

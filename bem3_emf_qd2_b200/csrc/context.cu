@@ -1,0 +1,537 @@
+// context.cu -- device-resident problems (bem3_ctx_*) and the solve stage's host orchestration
+// (solve_bieq, d3qd2_src/d3qd2_solve_bieq.c:36-84).
+#include <math.h>
+#include <stdlib.h>
+
+struct bem3_ctx_s {
+  int dev = 0;
+  int MN = 0, Ne = 0, NN = 0, Nn = 0, ps = 0, nwaves = 0;
+  double lambda0 = 0.0;
+  bem3_qpd2 qd;
+  QPLattice L;
+  std::vector<int> nv;                 // [(Ne+1)]
+  std::vector<std::vector<int>> sid;   // per domain, signed ids
+  std::vector<double> kn;              // [2 (MN+1)]
+  std::vector<int> doff;               // domain-id lists: offsets [MN+2]
+  std::vector<int> eni_h, md_h, sd_h;  // host copies for the solve's index tables
+  int solver = 0;                      // 0 auto, 1 full 8 NN system, 2 reduced 4 NN system
+  DevBuf geo, md, sd, eni, knd, Ui, dUi, dEiz, dEie, pos0, rn, ed, waves, dlist, dsd;
+  DevBuf dsid[BEM3_MAXDOM];
+  DevBuf U[BEM3_MAXDOM], dU[BEM3_MAXDOM], E[BEM3_MAXDOM], H[BEM3_MAXDOM], dE[BEM3_MAXDOM], dH[BEM3_MAXDOM];
+  DevBuf status;
+};
+
+namespace {
+
+size_t bv4_bytes(int ne) { return (size_t)(ne + 1) * 4 * 4 * 16; }
+size_t bv3_bytes(int ne) { return (size_t)(ne + 1) * 4 * 3 * 16; }
+
+SolveDev solve_view(bem3_ctx c)
+{
+  SolveDev S;
+  memset(&S, 0, sizeof S);
+  S.MN = c->MN; S.NN = c->NN; S.Ne = c->Ne;
+  S.geo = c->geo.as<double>(); S.md = c->md.as<int>(); S.sd = c->sd.as<int>(); S.eni = c->eni.as<int>();
+  S.kn = c->knd.as<double>(); S.Ui = c->Ui.as<double>(); S.dUi = c->dUi.as<double>();
+  S.dEiz = c->dEiz.as<double>(); S.dEie = c->dEie.as<double>(); S.pos0 = c->pos0.as<int>();
+  S.ch_re = 0.0; S.ch_im = -c->lambda0 / (2.0 * QP_PI);  // lambda0 / (2 pi i)
+  for (int d = 0; d <= c->MN; d++) {
+    S.ne[d] = (int)c->sid[d].size();
+    S.sid_h[d] = c->dsid[d].as<int>();
+    S.U[d] = c->U[d].as<double>(); S.dU[d] = c->dU[d].as<double>(); S.E[d] = c->E[d].as<double>();
+    S.H_[d] = c->H[d].as<double>(); S.dE[d] = c->dE[d].as<double>(); S.dH_[d] = c->dH[d].as<double>();
+  }
+  return S;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) { if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev); }
+  ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+}  // namespace
+
+extern "C" int bem3_ctx_create(const bem3_problem* P, bem3_ctx* out)
+{
+  if (!P || !out || P->MN < 0 || P->MN + 1 > BEM3_MAXDOM || P->Ne <= 0 || P->NN <= 0 || P->Nn <= 0 || !P->rn ||
+      !P->ed || !P->md || !P->sd || !P->eni || !P->Ne_d || !P->sid || !P->kn || !P->Ui || !P->dUi || !P->dEiz ||
+      !P->dEie || (P->nwaves > 0 && !P->waves) || P->mesh.Ne != P->Ne)
+    return BEM3_ERR_ARG;
+  *out = nullptr;
+  bem3_ctx c = new bem3_ctx_s();
+  int rc = 0;
+  auto fail = [&](int e) { delete c; return e; };
+  cudaGetDevice(&c->dev);
+  c->MN = P->MN; c->Ne = P->Ne; c->NN = P->NN; c->Nn = P->Nn; c->ps = P->ps; c->nwaves = P->nwaves;
+  c->lambda0 = P->lambda0;
+  c->qd = P->qd;
+  memset(&c->L, 0, sizeof c->L);
+  if (P->ps == 1 && qp_lattice_init(c->L, P->qd.k, P->qd.vk[0], P->qd.vk[1], P->qd.vd1[0], P->qd.vd1[1], P->qd.vd2[0],
+                                    P->qd.vd2[1]) != 0)
+    return fail(BEM3_ERR_LATTICE);
+  const int Ne = P->Ne, MN = P->MN;
+  c->nv.assign(P->mesh.nv, P->mesh.nv + Ne + 1);
+  c->eni_h.assign(P->eni, P->eni + 4 * (size_t)(Ne + 1));
+  c->md_h.assign(P->md, P->md + Ne + 1);
+  c->sd_h.assign(P->sd, P->sd + Ne + 1);
+  c->kn.assign(P->kn, P->kn + 2 * (MN + 1));
+  c->sid.resize(MN + 1);
+  for (int d = 0; d <= MN; d++) {
+    if (P->Ne_d[d] <= 0 || !P->sid[d]) return fail(BEM3_ERR_ARG);
+    c->sid[d].assign(P->sid[d], P->sid[d] + P->Ne_d[d]);
+    for (int s : c->sid[d])
+      if (s == 0 || abs(s) > Ne) return fail(BEM3_ERR_ARG);
+  }
+  for (int e = 1; e <= Ne; e++) {
+    if (P->md[e] < 0 || P->md[e] > MN || P->sd[e] < 0 || P->sd[e] > MN) return fail(BEM3_ERR_ARG);
+    for (int v = 0; v < 4; v++)
+      if (P->ed[4 * e + v] < 0 || P->ed[4 * e + v] > P->Nn) return fail(BEM3_ERR_ARG);
+  }
+  std::vector<double> geo((size_t)(Ne + 1) * GEO_STRIDE);
+  if ((rc = bem3_pack_geometry(&P->mesh, geo.data()))) return fail(rc);
+  if ((rc = upload(c->geo, geo.data(), geo.size())) || (rc = upload(c->md, P->md, (size_t)Ne + 1)) ||
+      (rc = upload(c->sd, P->sd, (size_t)Ne + 1)) || (rc = upload(c->eni, P->eni, (size_t)(Ne + 1) * 4)) ||
+      (rc = upload(c->knd, P->kn, (size_t)2 * (MN + 1))) || (rc = upload(c->Ui, P->Ui, (size_t)(Ne + 1) * 32)) ||
+      (rc = upload(c->dUi, P->dUi, (size_t)(Ne + 1) * 32)) || (rc = upload(c->dEiz, P->dEiz, (size_t)(Ne + 1) * 24)) ||
+      (rc = upload(c->dEie, P->dEie, (size_t)(Ne + 1) * 24)) || (rc = upload(c->rn, P->rn, (size_t)(P->Nn + 1) * 3)) ||
+      (rc = upload(c->ed, P->ed, (size_t)(Ne + 1) * 4)))
+    return fail(rc);
+  if (P->nwaves > 0 && (rc = upload(c->waves, P->waves, (size_t)P->nwaves))) return fail(rc);
+  std::vector<int> pos0((size_t)Ne + 1, -1);
+  for (size_t s = 0; s < c->sid[0].size(); s++)
+    if (c->sid[0][s] > 0) pos0[c->sid[0][s]] = (int)s;
+  if ((rc = upload(c->pos0, pos0.data(), pos0.size()))) return fail(rc);
+  // domain-id lists: the positive ids of each domain, in list order, with their sub-domains
+  std::vector<int> dl, ds;
+  c->doff.assign(MN + 2, 0);
+  for (int d = 0; d <= MN; d++) {
+    c->doff[d] = (int)dl.size();
+    for (int s : c->sid[d])
+      if (s > 0) { dl.push_back(s); ds.push_back(P->sd[s]); }
+  }
+  c->doff[MN + 1] = (int)dl.size();
+  if (dl.empty()) return fail(BEM3_ERR_ARG);
+  if ((rc = upload(c->dlist, dl.data(), dl.size())) || (rc = upload(c->dsd, ds.data(), ds.size()))) return fail(rc);
+  for (int d = 0; d <= MN; d++) {
+    const int ne = (int)c->sid[d].size();
+    if ((rc = upload(c->dsid[d], c->sid[d].data(), (size_t)ne))) return fail(rc);
+    if (c->U[d].alloc(bv4_bytes(ne)) || c->dU[d].alloc(bv4_bytes(ne)) || c->E[d].alloc(bv3_bytes(ne)) ||
+        c->H[d].alloc(bv3_bytes(ne)) || c->dE[d].alloc(bv3_bytes(ne)) || c->dH[d].alloc(bv3_bytes(ne)))
+      return fail(BEM3_ERR_CUDA);
+    cudaMemset(c->U[d].p, 0, bv4_bytes(ne)); cudaMemset(c->dU[d].p, 0, bv4_bytes(ne));
+    cudaMemset(c->E[d].p, 0, bv3_bytes(ne)); cudaMemset(c->H[d].p, 0, bv3_bytes(ne));
+    cudaMemset(c->dE[d].p, 0, bv3_bytes(ne)); cudaMemset(c->dH[d].p, 0, bv3_bytes(ne));
+  }
+  if (c->status.alloc(sizeof(int))) return fail(BEM3_ERR_CUDA);
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(BEM3_ERR_CUDA);
+  *out = c;
+  return 0;
+}
+
+extern "C" void bem3_ctx_destroy(bem3_ctx c)
+{
+  if (!c) return;
+  DeviceGuard g(c->dev);
+  delete c;
+}
+
+extern "C" int bem3_ctx_get_bv(bem3_ctx c, bem3_bv* out)
+{
+  if (!c || !out) return BEM3_ERR_ARG;
+  DeviceGuard g(c->dev);
+  for (int d = 0; d <= c->MN; d++) {
+    const int ne = (int)c->sid[d].size();
+    if ((out[d].U && cudaMemcpy(out[d].U, c->U[d].p, bv4_bytes(ne), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (out[d].dU && cudaMemcpy(out[d].dU, c->dU[d].p, bv4_bytes(ne), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (out[d].E && cudaMemcpy(out[d].E, c->E[d].p, bv3_bytes(ne), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (out[d].H && cudaMemcpy(out[d].H, c->H[d].p, bv3_bytes(ne), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (out[d].dE && cudaMemcpy(out[d].dE, c->dE[d].p, bv3_bytes(ne), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (out[d].dH && cudaMemcpy(out[d].dH, c->dH[d].p, bv3_bytes(ne), cudaMemcpyDeviceToHost) != cudaSuccess))
+      return BEM3_ERR_CUDA;
+  }
+  return 0;
+}
+
+extern "C" int bem3_ctx_set_bv(bem3_ctx c, const bem3_bv* bv)
+{
+  if (!c || !bv) return BEM3_ERR_ARG;
+  DeviceGuard g(c->dev);
+  for (int d = 0; d <= c->MN; d++) {
+    const int ne = (int)c->sid[d].size();
+    if (!bv[d].U || !bv[d].dU || !bv[d].E || !bv[d].H || !bv[d].dE || !bv[d].dH) return BEM3_ERR_ARG;
+    if (cudaMemcpy(c->U[d].p, bv[d].U, bv4_bytes(ne), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->dU[d].p, bv[d].dU, bv4_bytes(ne), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->E[d].p, bv[d].E, bv3_bytes(ne), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->H[d].p, bv[d].H, bv3_bytes(ne), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->dE[d].p, bv[d].dE, bv3_bytes(ne), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->dH[d].p, bv[d].dH, bv3_bytes(ne), cudaMemcpyHostToDevice) != cudaSuccess)
+      return BEM3_ERR_CUDA;
+  }
+  return 0;
+}
+
+namespace {
+
+// Column-major LU factorisation and solves (cuSOLVER), workspace and pivots owned by the caller.
+int lu_factor_cm(cusolverDnHandle_t h, double* A, int n, DevBuf& ipiv)
+{
+  int lwork = 0;
+  if (cusolverDnZgetrf_bufferSize(h, n, n, (cuDoubleComplex*)A, n, &lwork) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_SOLVE;
+  DevBuf work, info;
+  if (work.alloc(sizeof(cuDoubleComplex) * (size_t)(lwork > 0 ? lwork : 1)) || ipiv.alloc(sizeof(int) * (size_t)n) ||
+      info.alloc(sizeof(int)))
+    return BEM3_ERR_CUDA;
+  if (cusolverDnZgetrf(h, n, n, (cuDoubleComplex*)A, n, work.as<cuDoubleComplex>(), ipiv.as<int>(), info.as<int>()) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return BEM3_ERR_SOLVE;
+  int hinfo = 0;
+  if (cudaMemcpy(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return BEM3_ERR_CUDA;
+  return hinfo == 0 ? 0 : BEM3_ERR_SOLVE;
+}
+
+int lu_solve_cm(cusolverDnHandle_t h, const double* A, int n, DevBuf& ipiv, double* B, int nrhs)
+{
+  DevBuf info;
+  if (info.alloc(sizeof(int))) return BEM3_ERR_CUDA;
+  if (cusolverDnZgetrs(h, CUBLAS_OP_N, n, nrhs, (const cuDoubleComplex*)A, n, ipiv.as<int>(), (cuDoubleComplex*)B, n,
+                       info.as<int>()) != CUSOLVER_STATUS_SUCCESS)
+    return BEM3_ERR_SOLVE;
+  int hinfo = 0;
+  if (cudaMemcpy(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return BEM3_ERR_CUDA;
+  return hinfo == 0 ? 0 : BEM3_ERR_SOLVE;
+}
+
+int zgemm_nn(cublasHandle_t hb, int m, int n, int k, const double* A, int lda, const double* B, int ldb, double beta,
+             double* C, int ldc)
+{
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), bt = make_cuDoubleComplex(beta, 0.0);
+  return cublasZgemm(hb, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &one, (const cuDoubleComplex*)A, lda,
+                     (const cuDoubleComplex*)B, ldb, &bt, (cuDoubleComplex*)C, ldc) == CUBLAS_STATUS_SUCCESS
+             ? 0
+             : BEM3_ERR_SOLVE;
+}
+
+unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// Two-colouring of the domain graph (an edge per element between its two domains); the class of
+// domain 0 is eliminated.  Returns false when the graph is not bipartite.
+bool colour_domains(bem3_ctx c, std::vector<int>& elim)
+{
+  const int MN = c->MN;
+  std::vector<std::vector<int>> adj(MN + 1);
+  for (int e = 1; e <= c->Ne; e++) {
+    adj[c->md_h[e]].push_back(c->sd_h[e]);
+    adj[c->sd_h[e]].push_back(c->md_h[e]);
+  }
+  std::vector<int> col(MN + 1, -1);
+  for (int s = 0; s <= MN; s++) {
+    if (col[s] >= 0) continue;
+    col[s] = 0;
+    std::vector<int> st{s};
+    while (!st.empty()) {
+      int u = st.back();
+      st.pop_back();
+      for (int v : adj[u]) {
+        if (v == u) return false;
+        if (col[v] < 0) { col[v] = 1 - col[u]; st.push_back(v); }
+        else if (col[v] == col[u]) return false;
+      }
+    }
+  }
+  elim.assign(MN + 1, 0);
+  for (int d = 0; d <= MN; d++) elim[d] = (col[d] == col[0]);
+  return true;
+}
+
+// Reduced solve; fills X (device, 8 NN: U then dU, component-major, global node order).
+// Returns 0, 1 when the domain graph does not allow it, or an error code.
+int dtn_solve(bem3_ctx c, SolveDev& S, double* X)
+{
+  const int MN = c->MN, NN = c->NN;
+  std::vector<int> elim;
+  if (!colour_domains(c, elim)) return 1;
+  std::vector<DtnNode> nodes((size_t)NN);
+  std::vector<int> seen((size_t)NN, 0);
+  std::vector<std::vector<int>> gnode(MN + 1), cmap(MN + 1);
+  for (int d = 0; d <= MN; d++) {
+    for (int t = 0; t < S.ne[d]; t++) {
+      const int a = abs(c->sid[d][t]);
+      for (int tn = 0; tn < c->nv[a]; tn++) {
+        const int g = c->eni_h[4 * a + tn];
+        if (g < 0 || g >= NN) return BEM3_ERR_ARG;
+        const int j = (int)gnode[d].size();
+        gnode[d].push_back(g);
+        cmap[d].push_back(4 * t + tn);
+        DtnNode& q = nodes[g];
+        q.elem = a; q.l = tn;
+        if (elim[d]) { q.de = d; q.le = j; seen[g] |= 1; }
+        else { q.dn = d; q.ln = j; seen[g] |= 2; }
+      }
+    }
+  }
+  for (int g = 0; g < NN; g++)
+    if (seen[g] != 3) return 1;
+  int rc;
+  DevBuf dnodes;
+  if ((rc = upload(dnodes, nodes.data(), nodes.size()))) return rc;
+  DevBuf dg[BEM3_MAXDOM], dc[BEM3_MAXDOM];
+  for (int d = 0; d <= MN; d++)
+    if ((rc = upload(dg[d], gnode[d].data(), gnode[d].size())) || (rc = upload(dc[d], cmap[d].data(), cmap[d].size())))
+      return rc;
+  DtnArgs A;
+  A.node = dnodes.as<DtnNode>(); A.geo = S.geo; A.md = S.md; A.sd = S.sd; A.kn = S.kn; A.NN = NN;
+
+  cusolverDnHandle_t hs = nullptr;
+  cublasHandle_t hb = nullptr;
+  if (cusolverDnCreate(&hs) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
+  if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) { cusolverDnDestroy(hs); return BEM3_ERR_CUDA; }
+  struct Handles {
+    cusolverDnHandle_t s; cublasHandle_t b;
+    ~Handles() { cublasDestroy(b); cusolverDnDestroy(s); }
+  } handles{hs, hb};
+
+  // ---- eliminated domains: K_d = G_d^-1 H_d, g^d = G_d^-1 b^d
+  DevBuf Kd[BEM3_MAXDOM], gd[BEM3_MAXDOM];
+  KPtrs KP, GP;
+  memset(&KP, 0, sizeof KP);
+  memset(&GP, 0, sizeof GP);
+  for (int d = 0; d <= MN; d++) {
+    if (!elim[d]) continue;
+    const int n = (int)gnode[d].size();
+    const int N = 4 * S.ne[d];
+    DevBuf Gc, ipiv;
+    if (Gc.alloc((size_t)n * n * 16) || Kd[d].alloc((size_t)n * n * 16) || gd[d].alloc((size_t)n * 4 * 16))
+      return BEM3_ERR_CUDA;
+    k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.G[d], N, dc[d].as<int>(), n, Gc.as<double>());
+    k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.H[d], N, dc[d].as<int>(), n, Kd[d].as<double>());
+    k_dtn_rhs<<<dim3(n, 4), 256>>>(S, d, dc[d].as<int>(), n, gd[d].as<double>());
+    if ((rc = lu_factor_cm(hs, Gc.as<double>(), n, ipiv))) return rc;
+    if ((rc = lu_solve_cm(hs, Gc.as<double>(), n, ipiv, Kd[d].as<double>(), n))) return rc;
+    if ((rc = lu_solve_cm(hs, Gc.as<double>(), n, ipiv, gd[d].as<double>(), 4))) return rc;
+    KP.K[d] = Kd[d].as<double>(); KP.n[d] = n;
+    GP.K[d] = gd[d].as<double>(); GP.n[d] = n;
+  }
+  // ---- kept domains: their rows of the reduced system
+  const long long na = 4LL * NN;
+  DevBuf Ared, rhs;
+  if (Ared.alloc((size_t)na * na * 16) || rhs.alloc((size_t)na * 16)) return BEM3_ERR_CUDA;
+  long long row0 = 0;
+  for (int e = 0; e <= MN; e++) {
+    if (elim[e]) continue;
+    const int n = (int)gnode[e].size();
+    const int N = 4 * S.ne[e];
+    DevBuf Gc, Hc, Kh, P, Q, b, Gh;
+    if (Gc.alloc((size_t)n * n * 16) || Hc.alloc((size_t)n * n * 16) || Kh.alloc((size_t)n * NN * 16) ||
+        P.alloc((size_t)n * NN * 16) || Q.alloc((size_t)n * NN * 16) || b.alloc((size_t)n * 4 * 16) ||
+        Gh.alloc((size_t)n * 4 * 16))
+      return BEM3_ERR_CUDA;
+    k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.G[e], N, dc[e].as<int>(), n, Gc.as<double>());
+    k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.H[e], N, dc[e].as<int>(), n, Hc.as<double>());
+    k_dtn_khat<<<nblk((long long)n * NN, 256), 256>>>(A, KP, dg[e].as<int>(), n, e, 0, Kh.as<double>());
+    if ((rc = zgemm_nn(hb, n, NN, n, Gc.as<double>(), n, Kh.as<double>(), n, 0.0, P.as<double>(), n))) return rc;
+    k_dtn_khat<<<nblk((long long)n * NN, 256), 256>>>(A, KP, dg[e].as<int>(), n, e, 1, Kh.as<double>());
+    if ((rc = zgemm_nn(hb, n, NN, n, Gc.as<double>(), n, Kh.as<double>(), n, 0.0, Q.as<double>(), n))) return rc;
+    k_dtn_rows<<<nblk(4LL * n * na, 256), 256>>>(A, e, dg[e].as<int>(), n, Hc.as<double>(), Gc.as<double>(),
+                                                 P.as<double>(), Q.as<double>(), Ared.as<double>(), na, row0);
+    k_dtn_rhs<<<dim3(n, 4), 256>>>(S, e, dc[e].as<int>(), n, b.as<double>());
+    k_dtn_ghat<<<nblk(4LL * n, 256), 256>>>(A, GP, dg[e].as<int>(), n, e, Gh.as<double>());
+    if ((rc = zgemm_nn(hb, n, 4, n, Gc.as<double>(), n, Gh.as<double>(), n, 1.0, b.as<double>(), n))) return rc;
+    // b is n x 4 column-major: exactly the reduced rows' order c n + j
+    if (cudaMemcpy(rhs.as<double>() + 2 * row0, b.p, (size_t)n * 4 * 16, cudaMemcpyDeviceToDevice) != cudaSuccess)
+      return BEM3_ERR_CUDA;
+    row0 += 4LL * n;
+  }
+  if (row0 != na) return BEM3_ERR_ARG;
+  {
+    DevBuf ipiv;
+    if ((rc = lu_factor_cm(hs, Ared.as<double>(), (int)na, ipiv))) return rc;
+    if ((rc = lu_solve_cm(hs, Ared.as<double>(), (int)na, ipiv, rhs.as<double>(), 1))) return rc;
+  }
+  // ---- dU from the eliminated domains' relations
+  for (int d = 0; d <= MN; d++) {
+    if (!elim[d]) continue;
+    const int n = (int)gnode[d].size();
+    DevBuf Ud, KU;
+    if (Ud.alloc((size_t)n * 4 * 16) || KU.alloc((size_t)n * 4 * 16)) return BEM3_ERR_CUDA;
+    k_dtn_gather_u<<<nblk(4LL * n, 256), 256>>>(dg[d].as<int>(), n, NN, rhs.as<double>(), Ud.as<double>());
+    if ((rc = zgemm_nn(hb, n, 4, n, Kd[d].as<double>(), n, Ud.as<double>(), n, 0.0, KU.as<double>(), n))) return rc;
+    k_dtn_du<<<nblk(n, 128), 128>>>(A, d, dg[d].as<int>(), n, KU.as<double>(), gd[d].as<double>(), rhs.as<double>(), X);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return BEM3_ERR_CUDA;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int bem3_ctx_set_solver(bem3_ctx c, int method)
+{
+  if (!c || method < 0 || method > 2) return BEM3_ERR_ARG;
+  c->solver = method;
+  return 0;
+}
+
+extern "C" int bem3_ctx_solve(bem3_ctx c)
+{
+  if (!c) return BEM3_ERR_ARG;
+  DeviceGuard g(c->dev);
+  const int MN = c->MN, NN = c->NN;
+  int rc = 0;
+  SolveDev S = solve_view(c);
+  // ---- assembly of every domain (kept for the system and the dE, dH step)
+  DevBuf dGm[BEM3_MAXDOM], dHm[BEM3_MAXDOM], ddG[BEM3_MAXDOM], ddH[BEM3_MAXDOM], ddF[BEM3_MAXDOM];
+  for (int d = 0; d <= MN; d++) {
+    const int ne = S.ne[d];
+    const size_t N = (size_t)4 * ne;
+    if (dGm[d].alloc(N * N * 16) || dHm[d].alloc(N * N * 16) || ddG[d].alloc(2 * N * N * 16) ||
+        ddH[d].alloc(2 * N * N * 16) || ddF[d].alloc(N * 3 * 8))
+      return BEM3_ERR_CUDA;
+    const int periodic = (d == 0 && c->ps == 1) ? 1 : 0;
+    rc = bem3_assemble_domain_dev(c->geo.as<double>(), c->Ne, c->dsid[d].as<int>(), ne, d, periodic, &c->qd,
+                                  c->kn[2 * d], c->kn[2 * d + 1], dGm[d].as<double>(), dHm[d].as<double>(),
+                                  ddG[d].as<double>(), ddH[d].as<double>(), ddF[d].as<double>(), nullptr);
+    if (rc) return rc;
+    S.G[d] = dGm[d].as<double>(); S.H[d] = dHm[d].as<double>();
+    S.dG[d] = ddG[d].as<double>(); S.dH[d] = ddH[d].as<double>(); S.dF[d] = ddF[d].as<double>();
+  }
+  // ---- global system of the potentials: reduced (4 NN) where the domain graph allows it, else
+  //      the reference's full system (8 NN, create_tmatrix_csr row order)
+  {
+    const long long na = (long long)8 * NN;
+    DevBuf X;
+    if (X.alloc((size_t)na * 16)) return BEM3_ERR_CUDA;
+    rc = (c->solver == 1) ? 1 : dtn_solve(c, S, X.as<double>());
+    if (rc == 1 && c->solver == 2) return BEM3_ERR_ARG;  // reduced system asked for but not applicable
+    if (rc == 1) {
+      std::vector<int4> rowmap;
+      rowmap.reserve((size_t)na);
+      for (int d = 0; d <= MN; d++)
+        for (int cid = 0; cid < 4; cid++)
+          for (int t = 0; t < S.ne[d]; t++) {
+            const int nv = c->nv[abs(c->sid[d][t])];
+            for (int tn = 0; tn < nv; tn++) rowmap.push_back(make_int4(d, cid, t, tn));
+          }
+      if ((long long)rowmap.size() != na) return BEM3_ERR_ARG;
+      DevBuf drow, dA;
+      if ((rc = upload(drow, rowmap.data(), rowmap.size()))) return rc;
+      if (dA.alloc((size_t)na * na * 16)) return BEM3_ERR_CUDA;
+      cudaMemset(dA.p, 0, (size_t)na * na * 16);
+      k_build_rows<<<(unsigned)na, 256>>>(S, drow.as<int4>(), dA.as<double>(), X.as<double>(), na);
+      if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
+      cusolverDnHandle_t h = nullptr;
+      if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
+      rc = lu_solve_rowmajor(h, dA.as<double>(), (int)na, X.as<double>(), 1);
+      cusolverDnDestroy(h);
+    }
+    if (rc) return rc;
+    for (int d = 0; d <= MN; d++) k_store_bv<<<(4 * S.ne[d] + 127) / 128, 128>>>(S, d, X.as<double>());
+  }
+  // ---- boundary fields E, H (interior domains, and the open-region side of their nodes)
+  for (int d = 1; d <= MN; d++) k_eh_interior<<<(4 * S.ne[d] * 32 + 255) / 256, 256>>>(S, d);
+  // ---- normal derivatives dE, dH per domain
+  cusolverDnHandle_t h = nullptr;
+  if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
+  for (int d = 0; d <= MN && rc == 0; d++) {
+    std::vector<int> cmap;
+    for (int t = 0; t < S.ne[d]; t++) {
+      const int nv = c->nv[abs(c->sid[d][t])];
+      for (int tn = 0; tn < nv; tn++) cmap.push_back(4 * t + tn);
+    }
+    const int nn = (int)cmap.size();
+    DevBuf dc, dAd, dBd;
+    if ((rc = upload(dc, cmap.data(), cmap.size()))) break;
+    if (dAd.alloc((size_t)nn * nn * 16) || dBd.alloc((size_t)nn * 6 * 16)) { rc = BEM3_ERR_CUDA; break; }
+    k_deh_system<<<nn, 256>>>(S, d, dc.as<int>(), nn, dAd.as<double>(), dBd.as<double>());
+    rc = lu_solve_rowmajor(h, dAd.as<double>(), nn, dBd.as<double>(), 6);
+    if (rc) break;
+    k_deh_store<<<(nn + 127) / 128, 128>>>(S, d, dc.as<int>(), nn, dBd.as<double>());
+  }
+  cusolverDnDestroy(h);
+  if (rc) return rc;
+  if (cudaDeviceSynchronize() != cudaSuccess) return BEM3_ERR_CUDA;
+  return 0;
+}
+
+namespace {
+
+FieldArgs field_view(bem3_ctx c)
+{
+  FieldArgs A;
+  memset(&A, 0, sizeof A);
+  A.geo = c->geo.as<double>(); A.rn = c->rn.as<double>(); A.ed = c->ed.as<int>();
+  A.MN = c->MN; A.ps = c->ps;
+  A.dlist = c->dlist.as<int>(); A.dsd = c->dsd.as<int>();
+  for (int d = 0; d <= c->MN + 1; d++) A.doff[d] = c->doff[d];
+  for (int d = 0; d <= c->MN; d++) {
+    A.ne[d] = (int)c->sid[d].size();
+    A.sid[d] = c->dsid[d].as<int>();
+    A.E[d] = c->E[d].as<double>(); A.dE[d] = c->dE[d].as<double>();
+    A.H[d] = c->H[d].as<double>(); A.dH[d] = c->dH[d].as<double>();
+    A.kn[2 * d] = c->kn[2 * d]; A.kn[2 * d + 1] = c->kn[2 * d + 1];
+  }
+  A.vk0 = c->qd.vk[0]; A.vk1 = c->qd.vk[1];
+  A.d1x = c->qd.vd1[0]; A.d1y = c->qd.vd1[1]; A.d2x = c->qd.vd2[0]; A.d2y = c->qd.vd2[1];
+  const double det = A.d1x * A.d2y - A.d2x * A.d1y;
+  A.i_detd = det != 0.0 ? 1.0 / det : 0.0;
+  A.waves = c->waves.as<bem3_wave>(); A.nwaves = c->nwaves;
+  return A;
+}
+
+int run_domain_id(bem3_ctx c, const FieldArgs& A, int n, const double* r, DevBuf& dr, DevBuf& ddid, DevBuf& dcell)
+{
+  int rc;
+  if ((rc = upload(dr, r, (size_t)3 * n))) return rc;
+  if (ddid.alloc(sizeof(int) * (size_t)n) || dcell.alloc(sizeof(int2) * (size_t)n)) return BEM3_ERR_CUDA;
+  k_domain_id<<<(unsigned)(((size_t)n * 32 + 255) / 256), 256>>>(A, n, dr.as<double>(), ddid.as<int>(),
+                                                                  dcell.as<int2>());
+  return cudaGetLastError() == cudaSuccess ? 0 : BEM3_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int bem3_ctx_domain_id(bem3_ctx c, int n, const double* r, int* did)
+{
+  if (!c || n < 0 || (n > 0 && (!r || !did))) return BEM3_ERR_ARG;
+  if (n == 0) return 0;
+  DeviceGuard g(c->dev);
+  FieldArgs A = field_view(c);
+  DevBuf dr, ddid, dcell;
+  int rc = run_domain_id(c, A, n, r, dr, ddid, dcell);
+  if (rc) return rc;
+  return cudaMemcpy(did, ddid.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : BEM3_ERR_CUDA;
+}
+
+extern "C" int bem3_ctx_field(bem3_ctx c, int n, const double* r, int type, int total, double* E, double* H, int* did)
+{
+  if (!c || n < 0 || (n > 0 && (!r || !E || !H)) || (type != 0 && type != 1)) return BEM3_ERR_ARG;
+  if (n == 0) return 0;
+  DeviceGuard g(c->dev);
+  FieldArgs A = field_view(c);
+  DevBuf dr, ddid, dcell, dE, dH;
+  int rc = run_domain_id(c, A, n, r, dr, ddid, dcell);
+  if (rc) return rc;
+  if (dE.alloc((size_t)n * 6 * sizeof(double)) || dH.alloc((size_t)n * 6 * sizeof(double))) return BEM3_ERR_CUDA;
+  cudaMemset(c->status.p, 0, sizeof(int));
+  k_field<<<(unsigned)n, FIELD_THREADS>>>(A, c->L, n, dr.as<double>(), ddid.as<int>(), dcell.as<int2>(), type,
+                                          total ? 1 : 0, dE.as<double>(), dH.as<double>(), c->status.as<int>());
+  if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
+  int hs = 0;
+  if (cudaMemcpy(&hs, c->status.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(E, dE.p, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(H, dH.p, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      (did && cudaMemcpy(did, ddid.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess))
+    return BEM3_ERR_CUDA;
+  return hs;
+}
+
+extern "C" int bem3_solve_bieq_arrays(const bem3_problem* P, bem3_bv* out)
+{
+  if (!out) return BEM3_ERR_ARG;
+  bem3_ctx c = nullptr;
+  int rc = bem3_ctx_create(P, &c);
+  if (rc) return rc;
+  rc = bem3_ctx_solve(c);
+  if (!rc) rc = bem3_ctx_get_bv(c, out);
+  bem3_ctx_destroy(c);
+  return rc;
+}

@@ -192,7 +192,7 @@ BEM_HD int accp_point(const Elem& e, const QPLattice& L, const double* rt, const
   double rdv0 = dot3(vR, v0) * i_aR, rdv1 = dot3(vR, v1) * i_aR;
   double Wdv0 = dot3(vW, v0), Wdv1 = dot3(vW, v1);
   QPVal g;
-  int err = qpgf_eval<QP_V1>(L, vR, g);
+  int err = qpgf_eval<QP_V1, true>(L, vR, g);
   cplx hn = g.dG[0] * vW[0] + g.dG[1] * vW[1] + g.dG[2] * vW[2];
   double N[4];
   double i3 = i_aR * i_aR * i_aR;

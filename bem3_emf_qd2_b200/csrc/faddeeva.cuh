@@ -79,7 +79,19 @@ extern unsigned long long bem_stat_w[3];
 // w(z) for Im z >= 0 (upper half plane incl. the real axis).  Kept out of line and not unrolled:
 // one small copy serves every call site, which keeps the lattice-sum kernels inside the
 // instruction cache.
-BEM_HD_NOINLINE cplx faddeeva_w_upper(double x, double y)
+// Complex reciprocal with one real division.  The denominators met below are well scaled
+// (|t| >= 8 in the continued fraction; |z^2 - t_n| bounded away from 0 and from overflow by the
+// node choice), so Smith's scaling is not needed there; the result differs from crecip in the
+// last bits only.
+BEM_HD cplx crecip_fast(cplx b)
+{
+  const double d = 1.0 / (b.re * b.re + b.im * b.im);
+  return mk(b.re * d, -b.im * d);
+}
+
+// FAST selects crecip_fast for the reciprocals of the continued fraction and of the node sum.
+template <bool FAST>
+BEM_HD_NOINLINE cplx faddeeva_w_upper_t(double x, double y)
 {
   const double r2 = x * x + y * y;
   if (r2 >= 64.0) {
@@ -88,8 +100,8 @@ BEM_HD_NOINLINE cplx faddeeva_w_upper(double x, double y)
     cplx z = mk(x, y);
     cplx t = z;
 #pragma unroll 1
-    for (int n = 20; n >= 1; n--) t = z - (0.5 * n) * crecip(t);
-    cplx q = crecip(t);
+    for (int n = 20; n >= 1; n--) t = z - (0.5 * n) * (FAST ? crecip_fast(t) : crecip(t));
+    cplx q = FAST ? crecip_fast(t) : crecip(t);
     return mk(-FAD_INV_SQRTPI * q.im, FAD_INV_SQRTPI * q.re);  // i q / sqrt(pi)
   }
   if (r2 < 0.25) {
@@ -111,11 +123,17 @@ BEM_HD_NOINLINE cplx faddeeva_w_upper(double x, double y)
   cplx s = mk(0.0, 0.0);
   if (use_full) {
 #pragma unroll 1
-    for (int n = FAD_NFULL - 1; n >= 1; n--) s += fad_cfull[n] * crecip(mk(z2.re - fad_tfull[n], z2.im));
-    s = (2.0 * s) * z + crecip(z);
+    for (int n = FAD_NFULL - 1; n >= 1; n--) {
+      const cplx d = mk(z2.re - fad_tfull[n], z2.im);
+      s += fad_cfull[n] * (FAST ? crecip_fast(d) : crecip(d));
+    }
+    s = (2.0 * s) * z + (FAST ? crecip_fast(z) : crecip(z));
   } else {
 #pragma unroll 1
-    for (int n = FAD_NHALF - 1; n >= 0; n--) s += fad_chalf[n] * crecip(mk(z2.re - fad_thalf[n], z2.im));
+    for (int n = FAD_NHALF - 1; n >= 0; n--) {
+      const cplx d = mk(z2.re - fad_thalf[n], z2.im);
+      s += fad_chalf[n] * (FAST ? crecip_fast(d) : crecip(d));
+    }
     s = (2.0 * s) * z;
   }
   // (i h / pi) * s
@@ -128,11 +146,15 @@ BEM_HD_NOINLINE cplx faddeeva_w_upper(double x, double y)
   return w;
 }
 
+BEM_HD cplx faddeeva_w_upper(double x, double y) { return faddeeva_w_upper_t<false>(x, y); }
+
 // w(z) on the whole plane.
-BEM_HD cplx faddeeva_w(double x, double y)
+template <bool FAST>
+BEM_HD cplx faddeeva_w_t(double x, double y)
 {
-  if (y >= 0.0) return faddeeva_w_upper(x, y);
-  cplx wm = faddeeva_w_upper(-x, -y);
+  if (y >= 0.0) return faddeeva_w_upper_t<FAST>(x, y);
+  cplx wm = faddeeva_w_upper_t<FAST>(-x, -y);
   cplx e = cexp_(mk(y * y - x * x, -2.0 * x * y));  // e^{-z^2}
   return mk(2.0 * e.re - wm.re, 2.0 * e.im - wm.im);
 }
+BEM_HD cplx faddeeva_w(double x, double y) { return faddeeva_w_t<false>(x, y); }

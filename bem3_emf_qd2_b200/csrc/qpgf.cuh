@@ -36,6 +36,7 @@
 #define QP_EW_EXPM 3.0
 #define QP_EFS 0.1
 #define QP_MEPS 1.0e-15
+#define QP_PROP_CAP 2048  // most propagating orders a hoisted lattice list holds
 #define QP_PI 3.14159265358979323846
 #define QP_INV_SQRTPI 5.6418958354775628695e-1
 
@@ -57,6 +58,14 @@ struct QPLattice {
   int ew_only;           // 1 when bNp>0 || bNm>0 (always Ewald)
   int nc1;               // round(k||.d1 / 2 pi)
   cplx eb2;              // e^{i k||.d2}: Bloch phase step along d2 in the real-space sum
+  const struct QPProp* prop;  // propagating spectral orders (qp_prop_list), memory of the caller's side
+  int nprop;                  // their number (-1: no list); used by qpgf_eval<MODE, true> only
+};
+
+// One propagating spectral order n = (n1, n2): a_n = -k|| + n1 g1 + n2 g2 with beta_n^2 =
+// k^2 - |a_n|^2 > 0.  The set depends on the lattice and incidence only, not on the point.
+struct QPProp {
+  double an0, an1, bn2, bn;
 };
 
 struct QPVal {
@@ -85,6 +94,7 @@ extern unsigned long long bem_stat_t[5];  // real-space, spectral prop., spectra
 // Ewald real-space term (d3_qpgf_d2.c:1814-1838).  F and dF[3] (dF[2] still lacks the
 // factor -z/(4 pi) that the sum applies at the end).  ce = e^{i k||.R_l} is supplied by the
 // caller, which advances it along a row by one complex multiply per term instead of a sincos.
+template <bool FAST = false>
 BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1, int l2, cplx ce, cplx& F, cplx* dF)
 {
   BEM_STAT_T(0);
@@ -97,7 +107,7 @@ BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1
   double i_ve = 1.0 / veps;
   double rl_2e = rl * 0.5 * i_ve;
   double ef = exp(ke * ke - rl_2e * rl_2e);
-  cplx w = faddeeva_w(ke, rl_2e);
+  cplx w = faddeeva_w_t<FAST>(ke, rl_2e);
   double cfr = i_rl * i_rl * ef * (i_rl * w.re - L.k * w.im + i_ve * QP_INV_SQRTPI);
   cplx cf = ce * cfr;
   F = ce * (i_rl * ef * w.re);
@@ -106,66 +116,82 @@ BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1
   dF[2] = cf;
 }
 
-// Ewald spectral term (d3_qpgf_d2.c:1965-2009).  Returns 0 propagating, 1 evanescent,
-// -3 when beta_n == 0 exactly.  ce = e^{i a_n.r} comes from the caller's row recurrence.
+// Ewald spectral term (d3_qpgf_d2.c:1965-2009), propagating (beta_n^2 > 0, bn = beta_n) and
+// evanescent (beta_n^2 < 0, bn = |beta_n|) forms.  ce = e^{i a_n.r}.
+template <bool FAST = false>
+BEM_HD void qp_ew2_prop(const double* r, double veps, double an0, double an1, double bn2, double bn, cplx ce, cplx& F,
+                        cplx* dF)
+{
+  BEM_STAT_T(1);
+  double azve = r[2] / (2.0 * veps);
+  double ef = exp(bn2 * veps * veps - azve * azve);
+  cplx ff = expi(bn * r[2]);
+  cplx w = faddeeva_w_t<FAST>(bn * veps, azve);
+  // Fn = 2 ce / bn (i ef Im w + ff)
+  cplx t = mk(ff.re, ef * w.im + ff.im);
+  F = mk(2.0 * ce.re / bn, 2.0 * ce.im / bn) * t;
+  dF[0] = F * an0;
+  dF[1] = F * an1;
+  dF[2] = 2.0 * (ce * mk(ef * w.re - ff.re, -ff.im));
+}
+BEM_HD void qp_ew2_evan(const double* r, double veps, double an0, double an1, double bn, cplx ce, cplx& F, cplx* dF)
+{
+  BEM_STAT_T(2);
+  double azve = r[2] / (2.0 * veps);
+  double ebz = exp(bn * r[2]);
+  double f1 = ebz * erfc(bn * veps + azve);
+  double f2 = 1.0 / ebz * erfc(bn * veps - azve);
+  // Fn = ce / (i bn) (f1 + f2) = -i ce (f1+f2)/bn
+  F = mul_mi(ce * ((f1 + f2) / bn));
+  dF[0] = F * an0;
+  dF[1] = F * an1;
+  dF[2] = ce * (f1 - f2);
+}
+// Returns 0 propagating, 1 evanescent, -3 when beta_n == 0 exactly.
+template <bool FAST = false>
 BEM_HD int qp_ew2_term(const QPLattice& L, const double* r, double veps, int n1, int n2, cplx ce, cplx& F, cplx* dF)
 {
   double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
   double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
   double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
   if (bn2 > 0.0) {
-    BEM_STAT_T(1);
-    double bn = sqrt(bn2);
-    double azve = r[2] / (2.0 * veps);
-    double ef = exp(bn2 * veps * veps - azve * azve);
-    cplx ff = expi(bn * r[2]);
-    cplx w = faddeeva_w(bn * veps, azve);
-    // Fn = 2 ce / bn (i ef Im w + ff)
-    cplx t = mk(ff.re, ef * w.im + ff.im);
-    F = mk(2.0 * ce.re / bn, 2.0 * ce.im / bn) * t;
-    dF[0] = F * an0;
-    dF[1] = F * an1;
-    dF[2] = 2.0 * (ce * mk(ef * w.re - ff.re, -ff.im));
+    qp_ew2_prop<FAST>(r, veps, an0, an1, bn2, sqrt(bn2), ce, F, dF);
     return 0;
   } else if (bn2 < 0.0) {
-    BEM_STAT_T(2);
-    double bn = sqrt(-bn2);
-    double azve = r[2] / (2.0 * veps);
-    double ebz = exp(bn * r[2]);
-    double f1 = ebz * erfc(bn * veps + azve);
-    double f2 = 1.0 / ebz * erfc(bn * veps - azve);
-    // Fn = ce / (i bn) (f1 + f2) = -i ce (f1+f2)/bn
-    F = mul_mi(ce * ((f1 + f2) / bn));
-    dF[0] = F * an0;
-    dF[1] = F * an1;
-    dF[2] = ce * (f1 - f2);
+    qp_ew2_evan(r, veps, an0, an1, sqrt(-bn2), ce, F, dF);
     return 1;
   }
   return -3;
 }
 
-// Fourier-domain term (d3_qpgf_d2.c:856-885).  Returns 0 propagating, 1 evanescent, -2 if beta_n==0.
-// ph = e^{i a_n.r} comes from the caller's row recurrence.
+// Fourier-domain term (d3_qpgf_d2.c:856-885), propagating and evanescent forms; ph = e^{i a_n.r}.
+BEM_HD void qp_fd_prop(const double* r, double an0, double an1, double bn, cplx ph, cplx& F, cplx* dF)
+{
+  BEM_STAT_T(3);
+  dF[2] = ph * expi(bn * fabs(r[2]));
+  F = dF[2] * (1.0 / bn);
+  dF[0] = F * an0;
+  dF[1] = F * an1;
+}
+BEM_HD void qp_fd_evan(const double* r, double an0, double an1, double bn, cplx ph, cplx& F, cplx* dF)
+{
+  BEM_STAT_T(4);
+  dF[2] = ph * exp(-bn * fabs(r[2]));
+  F = mul_mi(dF[2] * (1.0 / bn));
+  dF[0] = F * an0;
+  dF[1] = F * an1;
+}
+// Returns 0 propagating, 1 evanescent, -2 if beta_n == 0.
 BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx ph, cplx& F, cplx* dF)
 {
   double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
   double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
   double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
   if (bn2 > 0.0) {
-    BEM_STAT_T(3);
-    double bn = sqrt(bn2);
-    dF[2] = ph * expi(bn * fabs(r[2]));
-    F = dF[2] * (1.0 / bn);
-    dF[0] = F * an0;
-    dF[1] = F * an1;
+    qp_fd_prop(r, an0, an1, sqrt(bn2), ph, F, dF);
     return 0;
   } else if (bn2 < 0.0) {
-    BEM_STAT_T(4);
-    double bn = sqrt(-bn2);
-    dF[2] = ph * exp(-bn * fabs(r[2]));
-    F = mul_mi(dF[2] * (1.0 / bn));
-    dF[0] = F * an0;
-    dF[1] = F * an1;
+    qp_fd_evan(r, an0, an1, sqrt(-bn2), ph, F, dF);
     return 1;
   }
   return -2;
@@ -181,8 +207,21 @@ BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx 
 // each term function has a single call site (small code, no instruction-cache thrash).
 
 // Ewald real-space sum (d3_qpgf_d2.c:1714-1812).  Returns the number of terms or -1.
-template <int MODE>
-BEM_HD int qp_ew1_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
+// Code-size knobs: the lattice sums and the whole evaluation can be compiled out of line
+// (fewer instruction-cache misses in the callers, at the price of a call).
+#if defined(QP_SUM_NOINLINE)
+#define QP_SUM_FN BEM_HD_NOINLINE
+#else
+#define QP_SUM_FN BEM_HD
+#endif
+#if defined(QP_EVAL_NOINLINE)
+#define QP_EVAL_FN BEM_HD_NOINLINE
+#else
+#define QP_EVAL_FN BEM_HD
+#endif
+
+template <int MODE, bool OPT = false>
+QP_SUM_FN int qp_ew1_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
 {
   S = mk(0, 0); dS[0] = mk(0, 0); dS[1] = mk(0, 0); dS[2] = mk(0, 0);
   cplx oS = S, od0 = S, od1 = S;
@@ -193,7 +232,7 @@ BEM_HD int qp_ew1_sum(const QPLattice& L, const double* r, double veps, double e
   for (;;) {
     const int l2 = lc + (side == 1 ? -off : off);
     cplx F, dF[3];
-    qp_ew1_term(L, r, veps, l1, l2, ce, F, dF);
+    qp_ew1_term<OPT>(L, r, veps, l1, l2, ce, F, dF);
     S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
     cc++;
     bool row_done = false;
@@ -245,17 +284,39 @@ BEM_HD int qp_ew1_sum(const QPLattice& L, const double* r, double veps, double e
 // returns terms or -2 / -3); FD == 1: Fourier-domain sum (d3_qpgf_d2.c:745-854, returns terms or
 // -1 / -2 / -4).  Row rule of the Ewald sum applies only to rows without propagating orders
 // beyond the centre (the reference's flg).
-template <int MODE, int FD>
-BEM_HD int qp_spec_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
+//
+// OPT: the propagating orders (a fixed set per lattice, L.prop) are summed first, in one loop
+// that every lane of a warp runs in step; the row walk then evaluates only evanescent orders and
+// passes over the propagating positions (they still count for the row rule).  The stop rules see
+// the propagating contributions earlier than the reference's order, so a sum may stop a term
+// sooner or later; every neglected term is still below the rule's relative threshold (1e-16 of
+// the running sum).  Without a list (L.nprop < 0) the sum runs in the reference's order.  OPT
+// also selects the division-light w(z) (faddeeva_w_t<true>).
+template <int MODE, int FD, bool OPT = false>
+QP_SUM_FN int qp_spec_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
 {
   if (FD && r[2] == 0.0) return -4;
   const int LIMIT = FD ? QP_FD_LIMIT : QP_EW_LIMIT;
   const int ELIM = FD ? -1 : -2;
   S = mk(0, 0); dS[0] = mk(0, 0); dS[1] = mk(0, 0); dS[2] = mk(0, 0);
-  cplx oS = S, od2 = S;
+  const bool hoist = OPT && L.nprop >= 0;
+  int cc = 0;
+  if (hoist) {
+#pragma unroll 1
+    for (int i = 0; i < L.nprop; i++) {
+      const QPProp q = L.prop[i];
+      const cplx ph = expi(q.an0 * r[0] + q.an1 * r[1]);
+      cplx F, dF[3];
+      if (FD) qp_fd_prop(r, q.an0, q.an1, q.bn, ph, F, dF);
+      else qp_ew2_prop<OPT>(r, veps, q.an0, q.an1, q.bn2, q.bn, ph, F, dF);
+      S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
+      cc++;
+    }
+  }
+  cplx oS = S, od2 = dS[2];
   const int nc = L.nc1;
   const cplx E2 = expi(L.g2x * r[0] + L.g2y * r[1]);  // phase step along n2
-  int cc = 0, dir = 0, n1 = nc, side = -1, off = 0, flg = 0;
+  int dir = 0, n1 = nc, side = -1, off = 0, flg = 0;
   int nc2;
   if (FD) nc2 = (int)round((L.vkx * L.g2x + L.vky * L.g2y - (double)n1 * L.g12) / L.g22);
   else nc2 = (int)round(-((-L.vkx + (double)n1 * L.g1x) * L.g2x + (-L.vky + (double)n1 * L.g1y) * L.g2y) / L.g22);
@@ -265,17 +326,35 @@ BEM_HD int qp_spec_sum(const QPLattice& L, const double* r, double veps, double 
   for (;;) {
     const int n2 = nc2 + (side == 1 ? -off : off);
     cplx F, dF[3];
-    int e = FD ? qp_fd_term(L, r, n1, n2, ph, F, dF) : qp_ew2_term(L, r, veps, n1, n2, ph, F, dF);
-    if (!FD) cc++;
+    int e;
+    if (hoist) {  // e == 2: a propagating order, already summed
+      const double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
+      const double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
+      const double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
+      if (bn2 > 0.0) {
+        e = 2;
+      } else if (bn2 < 0.0) {
+        if (FD) qp_fd_evan(r, an0, an1, sqrt(-bn2), ph, F, dF);
+        else qp_ew2_evan(r, veps, an0, an1, sqrt(-bn2), ph, F, dF);
+        e = 1;
+      } else {
+        e = FD ? -2 : -3;
+      }
+    } else {
+      e = FD ? qp_fd_term(L, r, n1, n2, ph, F, dF) : qp_ew2_term<OPT>(L, r, veps, n1, n2, ph, F, dF);
+    }
+    if (!FD && e != 2) cc++;
     if (e < 0) return e;
-    S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
-    if (FD) cc++;
+    if (e != 2) {
+      S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
+      if (FD) cc++;
+    }
     if (side < 0) {
       side = 0; off = 1; ph = ph0 * E2;
       continue;
     }
     bool stop = false;
-    if (e > 0) {
+    if (e == 1) {
       stop = qp_diff(dF[2], dS[2], eps);
       if (MODE == QP_BOTH) stop = stop && qp_diff(F, S, eps);
     } else {
@@ -336,8 +415,9 @@ BEM_HD int qp_spec_sum(const QPLattice& L, const double* r, double veps, double 
 // ---------------------------------------------------------------------------------------------
 // Full evaluation at r = (x, y, z): G and grad G.  Return value as the reference's
 // d3hm_qpgf_d2_v1: > 0 number of terms; -11..-14 FD errors; -21..-24 EW errors.
-template <int MODE>
-BEM_HD int qpgf_eval(const QPLattice& L, const double* r_in, QPVal& out)
+// OPT (the assembly kernels' form): hoisted propagating orders and the division-light w(z).
+template <int MODE, bool OPT = false>
+QP_EVAL_FN int qpgf_eval(const QPLattice& L, const double* r_in, QPVal& out)
 {
   const double eps = QP_MEPS;
   // lattice reduction (d3_qpgf_d2.c:417-423)
@@ -354,7 +434,7 @@ BEM_HD int qpgf_eval(const QPLattice& L, const double* r_in, QPVal& out)
   }
   int err;
   if (use_fd) {
-    err = qp_spec_sum<MODE, 1>(L, r, 0.0, eps, out.G, out.dG);
+    err = qp_spec_sum<MODE, 1, OPT>(L, r, 0.0, eps, out.G, out.dG);
     if (err < 0) return err - 10;
   } else {
     // split parameter (d3_qpgf_d2.c:1683-1693)
@@ -363,9 +443,9 @@ BEM_HD int qpgf_eval(const QPLattice& L, const double* r_in, QPVal& out)
     if (L.k * L.k * veps * veps - r2_min / (4.0 * veps * veps) > QP_EW_EXPM)
       veps = sqrt(QP_EW_EXPM + sqrt(L.k * L.k * r2_min + QP_EW_EXPM * QP_EW_EXPM)) / (sqrt(2.0) * L.k);
     cplx S2, dS2[3];
-    int c1 = qp_ew1_sum<MODE>(L, r, veps, eps, out.G, out.dG);
+    int c1 = qp_ew1_sum<MODE, OPT>(L, r, veps, eps, out.G, out.dG);
     if (c1 < 0) return c1 - 20;
-    int c2 = qp_spec_sum<MODE, 0>(L, r, veps, eps, S2, dS2);
+    int c2 = qp_spec_sum<MODE, 0, OPT>(L, r, veps, eps, S2, dS2);
     if (c2 < 0) return c2 - 20;
     out.G += S2; out.dG[0] += dS2[0]; out.dG[1] += dS2[1]; out.dG[2] += dS2[2];
     err = c1 + c2;
@@ -432,5 +512,29 @@ BEM_HD int qp_lattice_init(QPLattice& L, double k, double vkx, double vky, doubl
   }
   L.nc1 = n1;
   L.eb2 = expi(vkx * d2x + vky * d2y);
+  L.prop = nullptr;
+  L.nprop = -1;
   return 0;
+}
+
+// The propagating orders of a lattice in (n1, n2) order, with the term functions' expressions
+// for a_n and beta_n^2, over the window the row walks can reach (|n1 - nc1| < QP_EW_LIMIT, n2
+// within QP_EW_LIMIT of the row centre).  Returns their number, or -1 if more than cap.
+BEM_HD int qp_prop_list(const QPLattice& L, QPProp* out, int cap)
+{
+  int n = 0;
+  for (int n1 = L.nc1 - QP_EW_LIMIT + 1; n1 < L.nc1 + QP_EW_LIMIT; n1++) {
+    const int nc2 = (int)round(-((-L.vkx + (double)n1 * L.g1x) * L.g2x + (-L.vky + (double)n1 * L.g1y) * L.g2y) / L.g22);
+    for (int n2 = nc2 - QP_EW_LIMIT - 1; n2 <= nc2 + QP_EW_LIMIT + 1; n2++) {
+      const double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
+      const double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
+      const double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
+      if (bn2 > 0.0) {
+        if (n >= cap) return -1;
+        out[n].an0 = an0; out[n].an1 = an1; out[n].bn2 = bn2; out[n].bn = sqrt(bn2);
+        n++;
+      }
+    }
+  }
+  return n;
 }

@@ -342,121 +342,3 @@ int lu_solve_rowmajor(cusolverDnHandle_t h, double* A, int n, double* B, int nrh
 
 }  // namespace
 
-extern "C" int bem3_solve_bieq_arrays(const bem3_problem* P, bem3_bv* out)
-{
-  if (!P || !out || P->MN < 0 || P->MN + 1 > BEM3_MAXDOM || P->Ne <= 0 || P->NN <= 0) return BEM3_ERR_ARG;
-  const int MN = P->MN, Ne = P->Ne, NN = P->NN;
-  int rc;
-  // ---- inputs to the device
-  std::vector<double> geo((size_t)(Ne + 1) * GEO_STRIDE);
-  if ((rc = bem3_pack_geometry(&P->mesh, geo.data()))) return rc;
-  DevBuf dgeo, dmd, dsd, deni, dkn, dUi, ddUi, dEiz, dEie, dpos0;
-  DevBuf dsid[BEM3_MAXDOM], dGm[BEM3_MAXDOM], dHm[BEM3_MAXDOM], ddG[BEM3_MAXDOM], ddH[BEM3_MAXDOM], ddF[BEM3_MAXDOM];
-  DevBuf bU[BEM3_MAXDOM], bdU[BEM3_MAXDOM], bE[BEM3_MAXDOM], bH[BEM3_MAXDOM], bdE[BEM3_MAXDOM], bdH[BEM3_MAXDOM];
-  if ((rc = upload(dgeo, geo.data(), geo.size())) || (rc = upload(dmd, P->md, (size_t)Ne + 1)) ||
-      (rc = upload(dsd, P->sd, (size_t)Ne + 1)) || (rc = upload(deni, P->eni, (size_t)(Ne + 1) * 4)) ||
-      (rc = upload(dkn, P->kn, (size_t)2 * (MN + 1))) || (rc = upload(dUi, P->Ui, (size_t)(Ne + 1) * 32)) ||
-      (rc = upload(ddUi, P->dUi, (size_t)(Ne + 1) * 32)) || (rc = upload(dEiz, P->dEiz, (size_t)(Ne + 1) * 24)) ||
-      (rc = upload(dEie, P->dEie, (size_t)(Ne + 1) * 24)))
-    return rc;
-  std::vector<int> pos0((size_t)Ne + 1, -1);
-  for (int s = 0; s < P->Ne_d[0]; s++) {
-    int a = P->sid[0][s];
-    if (a > 0 && a <= Ne) pos0[a] = s;
-  }
-  if ((rc = upload(dpos0, pos0.data(), pos0.size()))) return rc;
-
-  SolveDev S;
-  memset(&S, 0, sizeof S);
-  S.MN = MN; S.NN = NN; S.Ne = Ne;
-  S.geo = dgeo.as<double>(); S.md = dmd.as<int>(); S.sd = dsd.as<int>(); S.eni = deni.as<int>();
-  S.kn = dkn.as<double>(); S.Ui = dUi.as<double>(); S.dUi = ddUi.as<double>();
-  S.dEiz = dEiz.as<double>(); S.dEie = dEie.as<double>(); S.pos0 = dpos0.as<int>();
-  const double two_pi = 2.0 * QP_PI;
-  S.ch_re = 0.0; S.ch_im = -P->lambda0 / two_pi;  // lambda0 / (2 pi i)
-
-  // ---- assembly of every domain (kept resident for the solve)
-  for (int d = 0; d <= MN; d++) {
-    const int ne = P->Ne_d[d];
-    const size_t N = (size_t)4 * ne;
-    S.ne[d] = ne;
-    if ((rc = upload(dsid[d], P->sid[d], (size_t)ne))) return rc;
-    if (dGm[d].alloc(N * N * 16) || dHm[d].alloc(N * N * 16) || ddG[d].alloc(2 * N * N * 16) ||
-        ddH[d].alloc(2 * N * N * 16) || ddF[d].alloc(N * 3 * 8))
-      return BEM3_ERR_CUDA;
-    int periodic = (d == 0 && P->ps == 1) ? 1 : 0;
-    rc = bem3_assemble_domain_dev(dgeo.as<double>(), Ne, dsid[d].as<int>(), ne, d, periodic, &P->qd, P->kn[2 * d],
-                                  P->kn[2 * d + 1], dGm[d].as<double>(), dHm[d].as<double>(), ddG[d].as<double>(),
-                                  ddH[d].as<double>(), ddF[d].as<double>(), nullptr);
-    if (rc) return rc;
-    S.sid_h[d] = dsid[d].as<int>();
-    S.G[d] = dGm[d].as<double>(); S.H[d] = dHm[d].as<double>();
-    S.dG[d] = ddG[d].as<double>(); S.dH[d] = ddH[d].as<double>(); S.dF[d] = ddF[d].as<double>();
-    const size_t nb4 = (size_t)(ne + 1) * 4 * 4 * 16, nb3 = (size_t)(ne + 1) * 4 * 3 * 16;
-    if (bU[d].alloc(nb4) || bdU[d].alloc(nb4) || bE[d].alloc(nb3) || bH[d].alloc(nb3) || bdE[d].alloc(nb3) ||
-        bdH[d].alloc(nb3))
-      return BEM3_ERR_CUDA;
-    cudaMemset(bU[d].p, 0, nb4); cudaMemset(bdU[d].p, 0, nb4);
-    cudaMemset(bE[d].p, 0, nb3); cudaMemset(bH[d].p, 0, nb3); cudaMemset(bdE[d].p, 0, nb3); cudaMemset(bdH[d].p, 0, nb3);
-    S.U[d] = bU[d].as<double>(); S.dU[d] = bdU[d].as<double>(); S.E[d] = bE[d].as<double>();
-    S.H_[d] = bH[d].as<double>(); S.dE[d] = bdE[d].as<double>(); S.dH_[d] = bdH[d].as<double>();
-  }
-
-  // ---- global system (create_tmatrix_csr row order) and its LU solve
-  std::vector<int4> rowmap;
-  rowmap.reserve((size_t)8 * NN);
-  for (int d = 0; d <= MN; d++)
-    for (int cid = 0; cid < 4; cid++)
-      for (int t = 0; t < P->Ne_d[d]; t++) {
-        int a = abs(P->sid[d][t]);
-        int nv = P->mesh.nv[a];
-        for (int tn = 0; tn < nv; tn++) rowmap.push_back(make_int4(d, cid, t, tn));
-      }
-  const long long na = (long long)8 * NN;
-  if ((long long)rowmap.size() != na) return BEM3_ERR_ARG;
-  DevBuf drow, dA, dB;
-  if ((rc = upload(drow, rowmap.data(), rowmap.size()))) return rc;
-  if (dA.alloc((size_t)na * na * 16) || dB.alloc((size_t)na * 16)) return BEM3_ERR_CUDA;
-  cudaMemset(dA.p, 0, (size_t)na * na * 16);
-  k_build_rows<<<(unsigned)na, 256>>>(S, drow.as<int4>(), dA.as<double>(), dB.as<double>(), na);
-  if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
-  cusolverDnHandle_t h = nullptr;
-  if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
-  rc = lu_solve_rowmajor(h, dA.as<double>(), (int)na, dB.as<double>(), 1);
-  if (rc) { cusolverDnDestroy(h); return rc; }
-  for (int d = 0; d <= MN; d++) k_store_bv<<<(4 * S.ne[d] + 127) / 128, 128>>>(S, d, dB.as<double>());
-  // ---- boundary fields E, H (interior domains, and the open-region side of their nodes)
-  for (int d = 1; d <= MN; d++) k_eh_interior<<<(4 * S.ne[d] * 32 + 255) / 256, 256>>>(S, d);
-  // ---- normal derivatives dE, dH per domain
-  for (int d = 0; d <= MN && rc == 0; d++) {
-    std::vector<int> cmap;
-    for (int t = 0; t < P->Ne_d[d]; t++) {
-      int nv = P->mesh.nv[abs(P->sid[d][t])];
-      for (int tn = 0; tn < nv; tn++) cmap.push_back(4 * t + tn);
-    }
-    const int nn = (int)cmap.size();
-    DevBuf dc, dAd, dBd;
-    if ((rc = upload(dc, cmap.data(), cmap.size()))) break;
-    if (dAd.alloc((size_t)nn * nn * 16) || dBd.alloc((size_t)nn * 6 * 16)) { rc = BEM3_ERR_CUDA; break; }
-    k_deh_system<<<nn, 256>>>(S, d, dc.as<int>(), nn, dAd.as<double>(), dBd.as<double>());
-    rc = lu_solve_rowmajor(h, dAd.as<double>(), nn, dBd.as<double>(), 6);
-    if (rc) break;
-    k_deh_store<<<(nn + 127) / 128, 128>>>(S, d, dc.as<int>(), nn, dBd.as<double>());
-  }
-  cusolverDnDestroy(h);
-  if (rc) return rc;
-  if (cudaDeviceSynchronize() != cudaSuccess) return BEM3_ERR_CUDA;
-  // ---- results back to the caller
-  for (int d = 0; d <= MN; d++) {
-    const int ne = S.ne[d];
-    const size_t nb4 = (size_t)(ne + 1) * 4 * 4 * 16, nb3 = (size_t)(ne + 1) * 4 * 3 * 16;
-    if ((out[d].U && cudaMemcpy(out[d].U, bU[d].p, nb4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
-        (out[d].dU && cudaMemcpy(out[d].dU, bdU[d].p, nb4, cudaMemcpyDeviceToHost) != cudaSuccess) ||
-        (out[d].E && cudaMemcpy(out[d].E, bE[d].p, nb3, cudaMemcpyDeviceToHost) != cudaSuccess) ||
-        (out[d].H && cudaMemcpy(out[d].H, bH[d].p, nb3, cudaMemcpyDeviceToHost) != cudaSuccess) ||
-        (out[d].dE && cudaMemcpy(out[d].dE, bdE[d].p, nb3, cudaMemcpyDeviceToHost) != cudaSuccess) ||
-        (out[d].dH && cudaMemcpy(out[d].dH, bdH[d].p, nb3, cudaMemcpyDeviceToHost) != cudaSuccess))
-      return BEM3_ERR_CUDA;
-  }
-  return 0;
-}

@@ -171,6 +171,25 @@ def read_gmsh(path: str, MN: int):
     return rn, ed, md, sd, gd
 
 
+def rotate_translate(rn: np.ndarray, rot) -> np.ndarray:
+    """rotation_translation_obj (d3qd2_src/d3qd2_setup.c:1110-1137): Rodrigues' rotation of every
+    node about the unit axis rv by th, then the translation tv, in the reference's operation order."""
+    rv0, rv1, rv2, th, tv0, tv1, tv2 = rot
+    a = math.sqrt(rv0 * rv0 + rv1 * rv1 + rv2 * rv2)
+    n0, n1, n2 = rv0 / a, rv1 / a, rv2 / a
+    st, ct = math.sin(th), math.cos(th)
+    M = [ct + n0 * n0 * (1.0 - ct), n0 * n1 * (1.0 - ct) - n2 * st, n2 * n0 * (1.0 - ct) + n1 * st,
+         n0 * n1 * (1.0 - ct) + n2 * st, ct + n1 * n1 * (1.0 - ct), n1 * n2 * (1.0 - ct) - n0 * st,
+         n2 * n0 * (1.0 - ct) - n1 * st, n1 * n2 * (1.0 - ct) + n0 * st, ct + n2 * n2 * (1.0 - ct)]
+    tv = (tv0, tv1, tv2)
+    out = np.array(rn, dtype=np.float64, copy=True)
+    for s in range(1, out.shape[0]):
+        x, y, z = rn[s, 0], rn[s, 1], rn[s, 2]
+        for i in range(3):
+            out[s, i] = M[3 * i] * x + M[3 * i + 1] * y + M[3 * i + 2] * z + tv[i]
+    return out
+
+
 def element_constants(rn: np.ndarray, ed: np.ndarray):
     """init_elem_const (d3qd2_src/d3qd2_setup.c:1139-1186), in the reference's operation order."""
     ne = ed.shape[0] - 1
@@ -212,7 +231,14 @@ ET34 = (-P34_N1, 0.0, P34_N1, 0.0)
 class Problem:
     """A loaded problem: the inputs the reference's solver holds in DQD2 (d3qd2_elem.h:49-60)."""
 
-    def __init__(self, waves, ps, vd1, vd2, media, rn, ed, md, sd, gd):
+    def __init__(self, waves, ps, vd1, vd2, media, rn, ed, md, sd, gd, rot=None):
+        """rot = (rv0, rv1, rv2, th, tv0, tv1, tv2): the optional rotation about axis rv by th and
+        translation tv that read_dqd2 takes from the command line (d3qd2_setup.c:16-38)."""
+        self.rot = tuple(float(x) for x in rot) if rot is not None else (1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+        if self.rot[3] != 0.0 or any(x != 0.0 for x in self.rot[4:]):
+            if self.rot[0] == 0.0 and self.rot[1] == 0.0 and self.rot[2] == 0.0:
+                raise ValueError("the vector defining the rotation axis is zero")
+            rn = rotate_translate(rn, self.rot)
         self.waves = waves
         self.ps = ps
         self.vd1, self.vd2 = vd1, vd2
@@ -295,13 +321,42 @@ class Problem:
         self.Ui[0] = 0
         self.dUi[0] = 0
 
+    def node_tangents(self):
+        """Unit tangents t_zeta, t_eta at every collocation node (tz_te_bd_node,
+        d3qd2_src/d3qd2_elem.c:122-143).  Returns two [(Ne+1), 4, 3] arrays (slot 0 zero)."""
+        cr = self.cr
+        quad = (self.nv == 4)[:, None, None]
+        et = np.asarray(ET44)[None, :, None]
+        zt = np.asarray(ZT44)[None, :, None]
+        vtz = cr[:, None, :, 1] + np.where(quad, cr[:, None, :, 3] * et, 0.0)
+        vte = cr[:, None, :, 2] + np.where(quad, cr[:, None, :, 3] * zt, 0.0)
+        vtz = vtz / np.linalg.norm(vtz, axis=-1, keepdims=True).clip(1e-300)
+        vte = vte / np.linalg.norm(vte, axis=-1, keepdims=True).clip(1e-300)
+        vtz[0] = 0
+        vte[0] = 0
+        return vtz, vte
+
+    def incident_tangent_derivatives(self):
+        """dE_inc/dt_zeta and dE_inc/dt_eta at every collocation node, summed over the incident
+        waves (calc_mipw_EH_dEHdv along tz_te_bd_node's tangents, as q1_solve_eh_bv does at
+        d3qd2_src/d3qd2_solve_bieq.c:1003-1004).  Returns two [(Ne+1), 4, 3] complex arrays."""
+        vtz, vte = self.node_tangents()
+        dEz = np.zeros((self.Ne + 1, 4, 3), np.complex128)
+        dEe = np.zeros_like(dEz)
+        for w in self.waves:
+            dEz += w.eh_dehdv(self.ren, vtz)[2]
+            dEe += w.eh_dehdv(self.ren, vte)[2]
+        dEz[0] = 0
+        dEe[0] = 0
+        return dEz, dEe
+
     @classmethod
-    def from_files(cls, ipw: str, ped: str, med: str, msh: str) -> "Problem":
+    def from_files(cls, ipw: str, ped: str, med: str, msh: str, rot=None) -> "Problem":
         waves = read_planewaves(ipw)
         ps, vd1, vd2 = read_periodicity(ped)
         media = read_media(med)
         rn, ed, md, sd, gd = read_gmsh(msh, len(media))
-        return cls(waves, ps, vd1, vd2, media, rn, ed, md, sd, gd)
+        return cls(waves, ps, vd1, vd2, media, rn, ed, md, sd, gd, rot=rot)
 
     # ---- arrays for the C ABI ------------------------------------------------------------
     def flat_mesh(self):
@@ -318,12 +373,15 @@ class Problem:
         return out
 
 
-def problem_to_arrays(waves, ps, vd1, vd2, media, rn, ed, md, sd, gd) -> dict:
+def problem_to_arrays(waves, ps, vd1, vd2, media, rn, ed, md, sd, gd, rot=None) -> dict:
     """Plain-array form of a problem's inputs (for fixtures and for meshes built in memory)."""
     wv = np.array([[w.lambda0, w.ni, w.power, w.e0x.real, w.e0x.imag, w.e0y.real, w.e0y.imag,
                     w.f[0], w.f[1], w.f[2], w.theta, w.phi] for w in waves])
-    return dict(waves=wv, ps=np.int32(ps), vd1=np.array(vd1, float), vd2=np.array(vd2, float),
-                media=np.array(media, np.complex128), rn=rn, ed=ed, md=md, sd=sd, gd=gd)
+    a = dict(waves=wv, ps=np.int32(ps), vd1=np.array(vd1, float), vd2=np.array(vd2, float),
+             media=np.array(media, np.complex128), rn=rn, ed=ed, md=md, sd=sd, gd=gd)
+    if rot is not None:
+        a["rot"] = np.array(rot, np.float64)
+    return a
 
 
 def problem_from_arrays(a: dict) -> Problem:
@@ -331,13 +389,59 @@ def problem_from_arrays(a: dict) -> Problem:
              for v in np.asarray(a["waves"])]
     return Problem(waves, int(a["ps"]), tuple(np.asarray(a["vd1"]).tolist()), tuple(np.asarray(a["vd2"]).tolist()),
                    [complex(x) for x in np.asarray(a["media"])], np.asarray(a["rn"]), np.asarray(a["ed"]),
-                   np.asarray(a["md"]), np.asarray(a["sd"]), np.asarray(a["gd"]))
+                   np.asarray(a["md"]), np.asarray(a["sd"]), np.asarray(a["gd"]),
+                   rot=np.asarray(a["rot"]).tolist() if "rot" in a else None)
 
 
-def load_inputs(ipw: str, ped: str, med: str, msh: str) -> dict:
-    """Reads the four reference input files into the plain-array form."""
+def load_inputs(ipw: str, ped: str, med: str, msh: str, rot=None) -> dict:
+    """Reads the four reference input files into the plain-array form; rot as Problem's."""
     waves = read_planewaves(ipw)
     ps, vd1, vd2 = read_periodicity(ped)
     media = read_media(med)
     rn, ed, md, sd, gd = read_gmsh(msh, len(media))
-    return problem_to_arrays(waves, ps, vd1, vd2, media, rn, ed, md, sd, gd)
+    return problem_to_arrays(waves, ps, vd1, vd2, media, rn, ed, md, sd, gd, rot)
+
+
+def write_input_files(a: dict, outdir: str, mesh_name: str = "mesh.msh"):
+    """Writes the plain-array form back as the reference's four input files (ipw, periodicity,
+    medium, Gmsh 2.2 mesh with every element twice, read_mesh_data's convention) and returns
+    their paths.  Reading them back with load_inputs gives the same arrays."""
+    import os
+    os.makedirs(outdir, exist_ok=True)
+    wv = np.asarray(a["waves"])
+    ipw = os.path.join(outdir, "ipw.txt")
+    with open(ipw, "w") as f:
+        f.write("## plane wave data\n# number of wave\n%d\n" % len(wv))
+        f.write("# lambda ni power real(e0x) imag(e0x) real(e0y) imag(e0y) fx fy fz theta phi\n")
+        for v in wv:
+            f.write(" ".join("%.17g" % x for x in v) + "\n")
+    ped = os.path.join(outdir, "periodicity_data.txt")
+    d1, d2 = np.asarray(a["vd1"]), np.asarray(a["vd2"])
+    with open(ped, "w") as f:
+        f.write("## periodicity datafile\n# periodicity_setting d1_x d1_y d2_x d2_y\n")
+        f.write("%d %.17g %.17g %.17g %.17g\n" % (int(a["ps"]), d1[0], d1[1], d2[0], d2[1]))
+    med = os.path.join(outdir, "medium_data.txt")
+    media = np.asarray(a["media"])
+    with open(med, "w") as f:
+        f.write("## medium datafile\n# number of medium\n%d\n# real imag\n" % len(media))
+        for m in media:
+            f.write("%.17g %.17g\n" % (m.real, m.imag))
+    msh = os.path.join(outdir, mesh_name)
+    rn, ed, md, sd, gd = (np.asarray(a[k]) for k in ("rn", "ed", "md", "sd", "gd"))
+    ne = ed.shape[0] - 1
+    with open(msh, "w") as f:
+        f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % (rn.shape[0] - 1))
+        for i in range(1, rn.shape[0]):
+            f.write("%d %.17g %.17g %.17g\n" % (i, rn[i, 0], rn[i, 1], rn[i, 2]))
+        f.write("$EndNodes\n$Elements\n%d\n" % (2 * ne))
+        for e in range(1, ne + 1):
+            tri = ed[e, 3] == 0
+            nodes = list(ed[e, :3]) if tri else list(ed[e])
+            rev = [nodes[0], nodes[2], nodes[1]] if tri else [nodes[0], nodes[3], nodes[2], nodes[1]]
+            et = 2 if tri else 3
+            tag1 = OPENDID if md[e] == 0 else int(md[e])
+            tag2 = OPENDID if sd[e] == 0 else int(sd[e])
+            f.write("%d %d 2 %d %d %s\n" % (2 * e - 1, et, tag1, gd[e], " ".join(str(int(x)) for x in nodes)))
+            f.write("%d %d 2 %d %d %s\n" % (2 * e, et, tag2, gd[e], " ".join(str(int(x)) for x in rev)))
+        f.write("$EndElements\n")
+    return ipw, ped, med, msh

@@ -125,6 +125,17 @@ int bem3_last_stats(bem3_stats *out);
  * FP64 roofline.  Runs a ~100 ms kernel. */
 double bem3_fp64_peak_tflops(void);
 
+/* One incident plane wave after set-up: the derived data IpwD and the translation of Ipw
+ * (d3qd2_src/ipw.h:19-37, filled by setup_ipw ipw.c:121-145).  Fields at x:
+ * E = E0 e exp(i ki k.(x - f)), H = E0 h exp(i ki k.(x - f)), k = (sin_t cos_p, sin_t sin_p, cos_t). */
+typedef struct {
+  double E0, ki;
+  double cos_t, sin_t, cos_p, sin_p;
+  double f[3];
+  double e[6]; /* ex, ey, ez complex */
+  double h[6]; /* hx, hy, hz complex */
+} bem3_wave;
+
 /* ---------------------------------------------------------------------------------------------
  * Boundary-integral equation solve.
  * Replaces solve_bieq (d3qd2_src/d3qd2_solve_bieq.c:36-84) on arrays: assembles every domain
@@ -148,6 +159,11 @@ typedef struct {
   double lambda0;
   const double *Ui, *dUi;   /* [(Ne+1)][4][4] complex incident potential and normal derivative */
   const double *dEiz, *dEie;/* [(Ne+1)][4][3] complex tangential derivatives of the incident E */
+  int Nn;                   /* mesh nodes (ids 1..Nn) */
+  const double *rn;         /* [(Nn+1)][3] node coordinates (BOUD.rn) */
+  const int *ed;            /* [(Ne+1)][4] element vertex node ids (BOUD.ed; ed[e][3] = 0 for triangles) */
+  int nwaves;
+  const bem3_wave *waves;   /* [nwaves] incident plane waves (MIPW) */
 } bem3_problem;
 
 /* Boundary values of one domain, same layout as SUBD (d3qd2_elem.h:13-20), slot 0 unused:
@@ -157,6 +173,43 @@ typedef struct {
 } bem3_bv;
 
 int bem3_solve_bieq_arrays(const bem3_problem *P, bem3_bv *out /* [MN+1] */);
+
+/* ---------------------------------------------------------------------------------------------
+ * Device-resident problem.  A context holds one problem's geometry, media, incident waves and
+ * boundary values on the current CUDA device, so that a solve and any number of field
+ * evaluations share one upload.  Contexts are independent of each other; one context must not
+ * be used from two threads at once. */
+typedef struct bem3_ctx_s *bem3_ctx;
+
+/* Copies the problem to the device.  The caller's arrays may be freed afterwards. */
+int bem3_ctx_create(const bem3_problem *P, bem3_ctx *out);
+void bem3_ctx_destroy(bem3_ctx c);
+
+/* solve_bieq on the device; the boundary values stay in the context. */
+int bem3_ctx_solve(bem3_ctx c);
+
+/* How bem3_ctx_solve solves the system of the potentials.  0 (default): eliminate dU through the
+ * Dirichlet-to-Neumann maps of one class of domains and solve the remaining 4 NN equations when the
+ * domains allow it (every element separates the two classes), else method 1.  1: the reference's
+ * system of 8 NN unknowns (create_tmatrix_csr, d3qd2_solve_bieq.c:258-282) as one dense LU.
+ * 2: the reduced system only (BEM3_ERR_ARG when not applicable).  No counterpart in the reference,
+ * which always solves the 8 NN system with PARDISO. */
+int bem3_ctx_set_solver(bem3_ctx c, int method);
+
+/* Boundary values to host arrays (layout of bem3_bv), or from host arrays (for example the
+ * values a reference result file holds, read by dat_read d3qd2_setup.c:300). */
+int bem3_ctx_get_bv(bem3_ctx c, bem3_bv *out /* [MN+1] */);
+int bem3_ctx_set_bv(bem3_ctx c, const bem3_bv *bv /* [MN+1] */);
+
+/* Domain of each point (q0_domain_id / domain_id, d3qd2_setup.c:157-238): did[n]. */
+int bem3_ctx_domain_id(bem3_ctx c, int n, const double *r, int *did);
+
+/* Electromagnetic field at n points (EH_s / EH_t, d3qd2_src/d3qd2_field.c:203-285).
+ * r: [n][3]; E, H: [n][3] complex; did: [n] domain of each point (may be NULL).
+ * type 0: nodal 4-point rules, type 1: 9-point (quads) / 7-point (triangles) rules.
+ * total != 0 adds the incident field in the open region (EH_t), else scattered/internal (EH_s).
+ * Points outside every domain get did = -1 and zero fields. */
+int bem3_ctx_field(bem3_ctx c, int n, const double *r, int type, int total, double *E, double *H, int *did);
 
 /* Gauss-Legendre nodes and weights on [-1, 1] (the reference's gauleg, com_src/gauleg.c:3). */
 void bem3_gauss_legendre(int n, double *x, double *w);

@@ -322,3 +322,11 @@ void rp_EH(int n, const double *r, int type, int total, double complex *E, doubl
 int rp_force(double *F, double *N, const double *rc, int type) { return force_FN(F, N, (double *)rc, type, &g_qd); }
 
 int rp_domain_id(const double *r) { return q0_domain_id((double *)r, &g_qd); }
+
+/* Field coefficients of source element sd (signed id) at point rt for domain did, as EH_s
+ * (d3qd2_field.c:229-231) computes them: q0_coef_rt in the periodic open region, coef_rt else. */
+void rp_coef_rt(int did, const double *rt, int sd, int type, double complex *CC)
+{
+  if (did == 0 && g_qd.bd.ps == 1) q0_coef_rt(CC, (double *)rt, sd, g_qd.kn[did], type, &(g_qd.bd));
+  else coef_rt(CC, (double *)rt, sd, g_qd.kn[did], type, &(g_qd.bd));
+}

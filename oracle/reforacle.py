@@ -74,6 +74,7 @@ class RefOracle:
         for f in (lib.rp_qpgf_v1, lib.rp_qpgf_qG, lib.rp_qpgf_dqG):
             f.argtypes = [C.c_int, _dp, _dp, C.c_double, _cp, _ip]
         lib.rp_faddeeva.argtypes = [C.c_int, _cp, C.c_double, _cp]
+        lib.rp_coef_rt.argtypes = [C.c_int, _dp, C.c_int, C.c_int, _cp]
         lib.rp_get_bv.argtypes = [C.c_int, _cp, _cp, _cp, _cp, _cp, _cp]
         lib.rp_set_bv.argtypes = [C.c_int, _cp, _cp, _cp, _cp, _cp, _cp]
         lib.rp_EH.argtypes = [C.c_int, _dp, C.c_int, C.c_int, _cp, _cp, _ip]
@@ -208,6 +209,12 @@ class RefOracle:
         F = np.zeros(3); N = np.zeros(3)
         self.lib.rp_force(F, N, np.asarray(rc, np.float64), type_)
         return F, N
+
+    def coef_rt(self, did: int, r, sd: int, type_: int) -> np.ndarray:
+        """CC[9] of source element sd at point r (EH_s's per-element coefficients)."""
+        out = np.zeros(9, np.complex128)
+        self.lib.rp_coef_rt(did, np.ascontiguousarray(r, np.float64), sd, type_, out)
+        return out
 
     def domain_id(self, r) -> int:
         return int(self.lib.rp_domain_id(np.asarray(r, np.float64)))

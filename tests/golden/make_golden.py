@@ -10,8 +10,13 @@ from its sources by oracle/Makefile and called through oracle/reforacle.py:
   rows_*.npz    inputs of a sample problem shipped with the reference (read by the reference's
                 own readers) and complete rows of create_cmatrix_domain
                 (d3qd2_src/d3qd2_solve_bieq.c:165-256) for selected collocation elements.
+  bv_*.npz      boundary values (U, dU, E, H, dE, dH of every domain) stored in the result files
+                the reference ships (verification/veri.dat, analysis_sample*/ex*.dat), read by its
+                own dat_read, plus the reference's EH_t (d3qd2_field.c) at probe points and its
+                force_FN (d3qd2_force.c) for those results, types 0 and 1.
 
-Usage: python tests/golden/make_golden.py [reference_dir]
+Usage: python tests/golden/make_golden.py [reference_dir] [section ...]
+       sections: gauleg faddeeva qpgf rows bv (default: all)
 """
 import os
 import sys
@@ -27,6 +32,8 @@ from reforacle import RefOracle  # noqa: E402
 from bem3_emf_qd2_b200.dqd2 import load_inputs  # noqa: E402
 
 REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+SECTIONS = {a for a in sys.argv[2:] if "=" not in a} or {"gauleg", "faddeeva", "qpgf", "rows", "bv"}
+ONLY = {x for a in sys.argv[2:] if a.startswith("only=") for x in a[5:].split(",")}
 
 
 def qpd_of(k, th, ph, d1, d2):
@@ -66,9 +73,52 @@ def gauleg_tables(o):
     np.savez_compressed(os.path.join(HERE, "gauleg.npz"), x12=g["xli"], w12=g["wli"], x64=g["xhi"], w64=g["whi"])
 
 
+# result files shipped with the reference: name -> (directory, .dat, mesh, rotation given to the
+# solver on its command line (d3qd2_bv_solver.log of each directory), probe points)
+BV_CASES = {
+    "veri": ("verification", "veri.dat", "sphere_m4.msh", None,
+             [(0.3, 0.0, 1.1), (0.0, 0.0, 0.0), (0.15, -0.1, 0.2), (0.9, 0.4, 0.05), (-0.5, 0.3, 1.5),
+              (0.1, -0.2, -1.3), (1.7, 1.2, 0.6)]),
+    "ex2": ("analysis_sample2", "ex2.dat", "cone_m1.msh", (1.0, 0.0, 0.0, 3.1415926535, 0.0, 0.0, 0.0),
+            [(0.3, 0.0, 1.1), (0.0, 0.0, 0.0), (0.3, 0.2, 1.2), (-0.4, 0.1, -1.0), (0.5, -0.6, 0.3)]),
+}
+
+
+def bv_fixtures(o):
+    for name, (sub, dat, msh, rot, pts) in BV_CASES.items():
+        if ONLY and name not in ONLY:
+            continue
+        d = os.path.join(REF, sub)
+        o.load_dat(os.path.join(d, dat))
+        files = [os.path.join(d, f) for f in ("ipw.txt", "periodicity_data.txt", "medium_data.txt", msh)]
+        rec = {"in/" + k: v for k, v in load_inputs(*files, rot=rot).items()}
+        rec["dat/rn"] = o.geometry()["rn"]  # the result file's (rotated) nodes, to pin the set-up
+        info = o.info()
+        for dd in range(info["MN"] + 1):
+            for k, v in o.boundary_values(dd).items():
+                rec[f"bv{dd}/{k}"] = v
+        r = np.array(pts, np.float64)
+        rec["probe/r"] = r
+        for ty in (0, 1):
+            E, H, did = o.EH(r, ty, total=True)
+            rec[f"probe/E{ty}"] = E
+            rec[f"probe/H{ty}"] = H
+            rec[f"probe/did"] = did
+            F, N = o.force((0.0, 0.0, 0.0), ty)
+            rec[f"force/F{ty}"] = F
+            rec[f"force/N{ty}"] = N
+        np.savez_compressed(os.path.join(HERE, f"bv_{name}.npz"), **rec)
+        print(name, "bv done", flush=True)
+
+
 def main():
     o = RefOracle()
-    gauleg_tables(o)
+    if "gauleg" in SECTIONS:
+        gauleg_tables(o)
+    if "bv" in SECTIONS:
+        bv_fixtures(o)
+    if not SECTIONS & {"faddeeva", "qpgf", "rows"}:
+        return
     rng = np.random.default_rng(20261203)
 
     # ---- Faddeeva -----------------------------------------------------------------------
@@ -77,7 +127,8 @@ def main():
         rng.uniform(-6, 6, 1000) + 1j * 10 ** rng.uniform(-12, 0.5, 1000) * rng.choice([-1, 1], 1000),
         rng.uniform(-0.5, 0.5, 500) + 1j * rng.uniform(-0.5, 0.5, 500),
     ])
-    np.savez_compressed(os.path.join(HERE, "faddeeva.npz"), z=z, w=o.faddeeva(z))
+    if "faddeeva" in SECTIONS:
+        np.savez_compressed(os.path.join(HERE, "faddeeva.npz"), z=z, w=o.faddeeva(z))
 
     # ---- QPGF -----------------------------------------------------------------------------
     out = {}
@@ -93,9 +144,12 @@ def main():
         out[name + "/ret_v1"] = rv1
         out[name + "/qG"] = g[:, 0]
         out[name + "/dqG"] = d
-    np.savez_compressed(os.path.join(HERE, "qpgf.npz"), **out)
+    if "qpgf" in SECTIONS:
+        np.savez_compressed(os.path.join(HERE, "qpgf.npz"), **out)
 
     # ---- rows of the assembly -----------------------------------------------------------
+    if "rows" not in SECTIONS:
+        return
     for name, (sub, msh, sel) in CASES.items():
         d = os.path.join(REF, sub)
         files = [os.path.join(d, f) for f in ("ipw.txt", "periodicity_data.txt", "medium_data.txt", msh)]

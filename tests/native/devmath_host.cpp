@@ -44,6 +44,9 @@ int hm_pair_regular(const double* geo, int td, int tn, int sd, int periodic, dou
 {
   QPLattice L;
   qp_lattice_init(L, p[0], p[1], p[2], p[4], p[5], p[6], p[7]);
+  static thread_local QPProp prop[QP_PROP_CAP];
+  L.nprop = qp_prop_list(L, prop, QP_PROP_CAP);
+  L.prop = prop;
   Elem et, es;
   load_elem(geo, td < 0 ? -td : td, et);
   load_elem(geo, sd < 0 ? -sd : sd, es);
@@ -131,4 +134,44 @@ int hm_self_periodic(const double* geo, int sd, int tn, const double* p, const d
   return err;
 }
 
+}
+
+#include "field.cuh"
+
+extern "C" {
+
+// Field coefficients of source element sd at point rt with the device rules (field.cuh);
+// out = CC[0..7] re/im pairs then F.  Returns the status of field_coef.
+int hm_field_coef(const double* geo, int sd, const double* rt, int periodic, double kre, double kim, int type,
+                  const double* p, double* out)
+{
+  QPLattice L;
+  qp_lattice_init(L, p[0], p[1], p[2], p[4], p[5], p[6], p[7]);
+  cplx CC[8];
+  double F;
+  int st = periodic ? field_coef<true>(geo, sd, rt, mk(kre, kim), type, L, CC, F)
+                    : field_coef<false>(geo, sd, rt, mk(kre, kim), type, L, CC, F);
+  for (int i = 0; i < 8; i++) { out[2 * i] = CC[i].re; out[2 * i + 1] = CC[i].im; }
+  out[16] = F;
+  return st;
+}
+
+// Solid angle of an element seen from rt (vertices rn[ed[e][v]]), as the domain search uses it.
+double hm_solid_angle(const double* rn, const int* ed, int e, int nv, const double* rt, int* flag)
+{
+  double rv[4][3];
+  for (int v = 0; v < 4; v++)
+    for (int k = 0; k < 3; k++) rv[v][k] = rn[3 * ed[4 * e + v] + k] - rt[k];
+  return solid_angle(nv, rv, *flag);
+}
+
+}
+
+extern "C" void hm_faddeeva_fast(int n, const double* z, double* w)
+{
+  for (int i = 0; i < n; i++) {
+    cplx v = faddeeva_w_t<true>(z[2 * i], z[2 * i + 1]);
+    w[2 * i] = v.re;
+    w[2 * i + 1] = v.im;
+  }
 }

@@ -30,12 +30,15 @@ def test_reference_oracle_reproduces_goldens():
 
 
 # ---- device math compiled for the host ------------------------------------------------------
-def test_faddeeva_host_build(devmath_host):
+@pytest.mark.parametrize("fast", [False, True])
+def test_faddeeva_host_build(devmath_host, fast):
+    """Both forms of w(z): Smith-scaled reciprocals (the QPGF entry point) and the
+    single-division reciprocals of the assembly kernels."""
     f = golden("faddeeva.npz")
     z = f["z"]
     zz = np.ascontiguousarray(np.stack([z.real, z.imag], 1).ravel())
     out = np.zeros_like(zz)
-    devmath_host.hm_faddeeva(len(z), zz.ctypes.data, out.ctypes.data)
+    (devmath_host.hm_faddeeva_fast if fast else devmath_host.hm_faddeeva)(len(z), zz.ctypes.data, out.ctypes.data)
     w = out[0::2] + 1j * out[1::2]
     # |w - w_ref| / |w_ref|: the reference itself targets 1e-15 relative error
     assert np.max(np.abs(w - f["w"]) / np.abs(f["w"])) < 1e-13
@@ -232,3 +235,33 @@ def test_self_pairs_host_build(devmath_host, case):
                 for name, dc in (("dG", c[9:13]), ("dH", c[13:17])):
                     ref = g[key.replace("/G", "/" + name)][2 * tn, cols]
                     assert np.abs(dc - ref).max() < 1e-11 * max(np.abs(ref).max(), 1e-300), (case, did, t, tn, name)
+
+
+# ---- the result-file fixtures against the reference's published run log ----------------------
+def test_veri_fixture_matches_reference_log():
+    """verification/example1.log of the reference prints, for its veri.dat, the total field at
+    (0.3, 0, 1.1) and the radiation force for types 0 and 1; the fixture (computed by the
+    reference's own code from the same veri.dat) must agree to the printed 15 digits (5e-14)."""
+    g = golden("bv_veri.npz")
+    r = g["probe/r"]
+    assert np.allclose(r[0], [0.3, 0.0, 1.1])
+    log = {  # verification/example1.log, lines 29-41
+        "E0": [-3.76208072827608e-02 - 2.85785594404603e-03j, 7.49983749571966e-03 + 7.41792296005539e-04j],
+        "H0": -5.13555625232993e-02 - 3.84820633916324e-03j,
+        "E1": [-3.76208144538066e-02 - 2.85786232985435e-03j, 7.49983744933408e-03 + 7.41786762174399e-04j],
+        "H1": -5.13555629477514e-02 - 3.84820673327311e-03j,
+        "F0": [2.26768049370030e-07, 1.53318582305794e-06],
+        "F1": [2.28388853685501e-07, 1.54144035834764e-06],
+        "N0y": -9.05416804491539e-11,
+        "N1y": -9.09514287537933e-11,
+    }
+    for ty in (0, 1):
+        E, H = g[f"probe/E{ty}"][0], g[f"probe/H{ty}"][0]
+        assert abs(E[0] - log[f"E{ty}"][0]) <= 5e-14 * abs(E[0])
+        assert abs(E[2] - log[f"E{ty}"][1]) <= 5e-14 * abs(E[2])
+        assert abs(H[1] - log[f"H{ty}"]) <= 5e-14 * abs(H[1])
+        F, N = g[f"force/F{ty}"], g[f"force/N{ty}"]
+        assert abs(F[0] - log[f"F{ty}"][0]) <= 5e-14 * abs(F[0])
+        assert abs(F[2] - log[f"F{ty}"][1]) <= 5e-14 * abs(F[2])
+        # the torque is a small difference of large moments: 12 of its printed digits agree
+        assert abs(N[1] - log[f"N{ty}y"]) <= 1e-11 * abs(N[1])
