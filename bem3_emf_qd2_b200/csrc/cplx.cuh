@@ -54,6 +54,13 @@ BEM_HD cplx expi(double a) {  // e^{i a}
 #endif
   return mk(c, s);
 }
+BEM_HD double rsqrt_(double x) {  // 1/sqrt(x)
+#if defined(__CUDA_ARCH__)
+  return rsqrt(x);
+#else
+  return 1.0 / sqrt(x);
+#endif
+}
 BEM_HD cplx cexp_(cplx z) {  // e^{z}
   double e = exp(z.re);
   cplx p = expi(z.im);

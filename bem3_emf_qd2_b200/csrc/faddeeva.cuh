@@ -94,6 +94,22 @@ template <bool FAST>
 BEM_HD_NOINLINE cplx faddeeva_w_upper_t(double x, double y)
 {
   const double r2 = x * x + y * y;
+  if (FAST && r2 >= 64.0 && r2 < 1.0e8) {
+    BEM_STAT_W(0);
+    // the same 20-level continued fraction by the forward (Wallis) recurrence of its numerators
+    // and denominators: f = A_20 / B_20 with A_k = z A_{k-1} - (k/2) A_{k-2} (B likewise), one
+    // division in all.  |A_k| ~ |z|^k stays far from overflow for |z| < 1e4.
+    const cplx z = mk(x, y);
+    cplx Am = mk(1.0, 0.0), A = z, Bm = mk(0.0, 0.0), B = mk(1.0, 0.0);
+#pragma unroll 1
+    for (int k = 1; k <= 20; k++) {
+      const double a = -0.5 * k;
+      const cplx An = z * A + a * Am, Bn = z * B + a * Bm;
+      Am = A; A = An; Bm = B; B = Bn;
+    }
+    const cplx q = B * crecip_fast(A);  // 1 / f
+    return mk(-FAD_INV_SQRTPI * q.im, FAD_INV_SQRTPI * q.re);
+  }
   if (r2 >= 64.0) {
     BEM_STAT_W(0);
     // continued fraction, 20 levels, bottom-up
@@ -121,7 +137,26 @@ BEM_HD_NOINLINE cplx faddeeva_w_upper_t(double x, double y)
   const cplx z = mk(x, y);
   const cplx z2 = z * z;
   cplx s = mk(0.0, 0.0);
-  if (use_full) {
+  if (FAST) {
+    // the node sum two terms at a time over a common denominator:
+    //   c_a/(w - t_a) + c_b/(w - t_b) = ((c_a + c_b) w - (c_a t_b + c_b t_a)) / (w^2 - (t_a + t_b) w + t_a t_b)
+    // (w = z^2), one division per pair
+    const double* c = use_full ? fad_cfull : fad_chalf;
+    const double* tt = use_full ? fad_tfull : fad_thalf;
+    const int lo = use_full ? 1 : 0;
+    const int hi = use_full ? FAD_NFULL - 1 : FAD_NHALF - 1;
+    const cplx w2 = z2 * z2;
+    int n = hi;
+#pragma unroll 1
+    for (; n - 1 >= lo; n -= 2) {
+      const double ca = c[n], cb = c[n - 1], ta = tt[n], tb = tt[n - 1];
+      const cplx D = mk(w2.re - (ta + tb) * z2.re + ta * tb, w2.im - (ta + tb) * z2.im);
+      const cplx N = mk((ca + cb) * z2.re - (ca * tb + cb * ta), (ca + cb) * z2.im);
+      s += N * crecip_fast(D);
+    }
+    if (n >= lo) s += c[n] * crecip_fast(mk(z2.re - tt[n], z2.im));
+    s = use_full ? (2.0 * s) * z + crecip_fast(z) : (2.0 * s) * z;
+  } else if (use_full) {
 #pragma unroll 1
     for (int n = FAD_NFULL - 1; n >= 1; n--) {
       const cplx d = mk(z2.re - fad_tfull[n], z2.im);

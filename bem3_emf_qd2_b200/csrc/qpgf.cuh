@@ -101,8 +101,15 @@ BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1
   double Rl0 = (double)l1 * L.d1x + (double)l2 * L.d2x;
   double Rl1 = (double)l1 * L.d1y + (double)l2 * L.d2y;
   double px = r[0] + Rl0, py = r[1] + Rl1;
-  double rl = sqrt(px * px + py * py + r[2] * r[2]);
-  double i_rl = 1.0 / rl;
+  double rl2 = px * px + py * py + r[2] * r[2];
+  double rl, i_rl;
+  if (FAST) {  // one reciprocal square root instead of a square root and a division
+    i_rl = rsqrt_(rl2);
+    rl = rl2 * i_rl;
+  } else {
+    rl = sqrt(rl2);
+    i_rl = 1.0 / rl;
+  }
   double ke = L.k * veps;
   double i_ve = 1.0 / veps;
   double rl_2e = rl * 0.5 * i_ve;
@@ -129,12 +136,14 @@ BEM_HD void qp_ew2_prop(const double* r, double veps, double an0, double an1, do
   cplx w = faddeeva_w_t<FAST>(bn * veps, azve);
   // Fn = 2 ce / bn (i ef Im w + ff)
   cplx t = mk(ff.re, ef * w.im + ff.im);
-  F = mk(2.0 * ce.re / bn, 2.0 * ce.im / bn) * t;
+  F = FAST ? (ce * (2.0 / bn)) * t : mk(2.0 * ce.re / bn, 2.0 * ce.im / bn) * t;
   dF[0] = F * an0;
   dF[1] = F * an1;
   dF[2] = 2.0 * (ce * mk(ef * w.re - ff.re, -ff.im));
 }
-BEM_HD void qp_ew2_evan(const double* r, double veps, double an0, double an1, double bn, cplx ce, cplx& F, cplx* dF)
+// ibn = 1/bn: the evaluation forms below differ only in how they obtain bn and 1/bn.
+BEM_HD void qp_ew2_evan(const double* r, double veps, double an0, double an1, double bn, double ibn, cplx ce, cplx& F,
+                        cplx* dF)
 {
   BEM_STAT_T(2);
   double azve = r[2] / (2.0 * veps);
@@ -142,7 +151,7 @@ BEM_HD void qp_ew2_evan(const double* r, double veps, double an0, double an1, do
   double f1 = ebz * erfc(bn * veps + azve);
   double f2 = 1.0 / ebz * erfc(bn * veps - azve);
   // Fn = ce / (i bn) (f1 + f2) = -i ce (f1+f2)/bn
-  F = mul_mi(ce * ((f1 + f2) / bn));
+  F = mul_mi(ce * ((f1 + f2) * ibn));
   dF[0] = F * an0;
   dF[1] = F * an1;
   dF[2] = ce * (f1 - f2);
@@ -158,7 +167,8 @@ BEM_HD int qp_ew2_term(const QPLattice& L, const double* r, double veps, int n1,
     qp_ew2_prop<FAST>(r, veps, an0, an1, bn2, sqrt(bn2), ce, F, dF);
     return 0;
   } else if (bn2 < 0.0) {
-    qp_ew2_evan(r, veps, an0, an1, sqrt(-bn2), ce, F, dF);
+    const double bn = sqrt(-bn2);
+    qp_ew2_evan(r, veps, an0, an1, bn, 1.0 / bn, ce, F, dF);
     return 1;
   }
   return -3;
@@ -173,11 +183,11 @@ BEM_HD void qp_fd_prop(const double* r, double an0, double an1, double bn, cplx 
   dF[0] = F * an0;
   dF[1] = F * an1;
 }
-BEM_HD void qp_fd_evan(const double* r, double an0, double an1, double bn, cplx ph, cplx& F, cplx* dF)
+BEM_HD void qp_fd_evan(const double* r, double an0, double an1, double bn, double ibn, cplx ph, cplx& F, cplx* dF)
 {
   BEM_STAT_T(4);
   dF[2] = ph * exp(-bn * fabs(r[2]));
-  F = mul_mi(dF[2] * (1.0 / bn));
+  F = mul_mi(dF[2] * ibn);
   dF[0] = F * an0;
   dF[1] = F * an1;
 }
@@ -191,7 +201,8 @@ BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx 
     qp_fd_prop(r, an0, an1, sqrt(bn2), ph, F, dF);
     return 0;
   } else if (bn2 < 0.0) {
-    qp_fd_evan(r, an0, an1, sqrt(-bn2), ph, F, dF);
+    const double bn = sqrt(-bn2);
+    qp_fd_evan(r, an0, an1, bn, 1.0 / bn, ph, F, dF);
     return 1;
   }
   return -2;
@@ -207,12 +218,13 @@ BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx 
 // each term function has a single call site (small code, no instruction-cache thrash).
 
 // Ewald real-space sum (d3_qpgf_d2.c:1714-1812).  Returns the number of terms or -1.
-// Code-size knobs: the lattice sums and the whole evaluation can be compiled out of line
-// (fewer instruction-cache misses in the callers, at the price of a call).
-#if defined(QP_SUM_NOINLINE)
-#define QP_SUM_FN BEM_HD_NOINLINE
-#else
+// Code-size knobs: the lattice sums are compiled out of line by default (measured faster: fewer
+// instruction-cache misses and smaller register demand in the element kernels); the whole
+// evaluation can be too.
+#if defined(QP_SUM_INLINE)
 #define QP_SUM_FN BEM_HD
+#else
+#define QP_SUM_FN BEM_HD_NOINLINE
 #endif
 #if defined(QP_EVAL_NOINLINE)
 #define QP_EVAL_FN BEM_HD_NOINLINE
@@ -334,8 +346,11 @@ QP_SUM_FN int qp_spec_sum(const QPLattice& L, const double* r, double veps, doub
       if (bn2 > 0.0) {
         e = 2;
       } else if (bn2 < 0.0) {
-        if (FD) qp_fd_evan(r, an0, an1, sqrt(-bn2), ph, F, dF);
-        else qp_ew2_evan(r, veps, an0, an1, sqrt(-bn2), ph, F, dF);
+        // 1/|beta_n| from one reciprocal square root, |beta_n| = -beta_n^2 / |beta_n|
+        const double ibn = rsqrt_(-bn2);
+        const double bn = -bn2 * ibn;
+        if (FD) qp_fd_evan(r, an0, an1, bn, ibn, ph, F, dF);
+        else qp_ew2_evan(r, veps, an0, an1, bn, ibn, ph, F, dF);
         e = 1;
       } else {
         e = FD ? -2 : -3;

@@ -346,7 +346,7 @@ BEM_HD int self_per_points(const SelfInfo& S, const QPLattice& L, const double* 
     }
     self_N(S, zeta, eta, N);
     QPVal g;
-    int e2 = qpgf_eval<QP_BOTH>(L, vR, g);
+    int e2 = qpgf_eval<QP_BOTH, true>(L, vR, g);
     if (e2 < 0) err = e2;
     double aW = S.bil ? vnorm3(W) : 1.0;
     cplx gw = g.G * (w * aW * r);

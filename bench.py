@@ -31,10 +31,12 @@ sys.path.insert(0, REPO)
 
 METRIC = "QPGF element-pair evals/s"
 UNIT = "pairs/s"
-# FP64 operations per lattice-sum term of the regular periodic kernel, hardware-counted
-# (2*DFMA + DADD + DMUL instructions / terms) with ncu on the sphere384 case; see
-# profiles/k_reg_periodic_sphere384.txt.  Used for the live FP64 roofline figure.
-FP64_OPS_PER_TERM = None
+# FP64 operations per lattice-sum term of the regular periodic kernel, per workload: the
+# FP64 instructions ncu counts in one launch (2 DFMA + DADD + DMUL, thread level) divided by the
+# terms the kernel's own counter reports for that launch, captured on the workload's /stride8
+# subsample (same lattice, wavelength and element size).  The live roofline figure is
+# terms/s x this number; the captures are summarised in profiles/.
+FP64_OPS_PER_TERM = {}
 
 
 def parse():
@@ -47,6 +49,9 @@ def parse():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline sampling")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--element-stride", type=int, default=1,
+                    help="keep every S-th element of each domain's list: a smaller workload with the "
+                         "same lattice, wavelength and element size, for profiler captures")
     return ap.parse_args()
 
 
@@ -203,6 +208,10 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     tmp = tempfile.mkdtemp(prefix=f"bem3_{rank}_")
     p, files = meshgen.problem(args.config, tmp)
+    workload = args.config
+    if args.element_stride > 1:
+        p.sid = [s[::args.element_stride].copy() for s in p.sid]
+        workload = f"{args.config}/stride{args.element_stride}"
     dev = B.DeviceProblem(p)
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
@@ -254,8 +263,9 @@ def run_ours(args):
     if reg_launches:
         per_launch_ms = reg_ms / reg_launches
         terms_per_launch = terms / reg_launches
-        if FP64_OPS_PER_TERM:
-            achieved = terms_per_launch * FP64_OPS_PER_TERM / (per_launch_ms * 1e-3) / 1e12
+        ops = FP64_OPS_PER_TERM.get(args.config)
+        if ops:
+            achieved = terms_per_launch * ops / (per_launch_ms * 1e-3) / 1e12
             roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": None,
                     "kernel": "k_reg_periodic", "peak_source": "measured DFMA probe on this GPU"}
@@ -302,7 +312,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cube-sphere meshes)",
-            "config": {"workload": args.config, "pairs_per_step": pairs, "domains": len(domains),
+            "config": {"workload": workload, "pairs_per_step": pairs, "domains": len(domains),
                        "elements": int(p.Ne), "gh_pairs_per_step": gh,
                        "l2": "each step writes %.1f GB of matrices (> 126 MB L2); no state carried in L2"
                              % (sum(16 * 6 * (4 * len(s)) ** 2 for s in p.sid) / 1e9),

@@ -119,6 +119,9 @@ int hm_self_periodic(const double* geo, int sd, int tn, const double* p, const d
 {
   QPLattice L;
   qp_lattice_init(L, p[0], p[1], p[2], p[4], p[5], p[6], p[7]);
+  static thread_local QPProp prop[QP_PROP_CAP];
+  L.nprop = qp_prop_list(L, prop, QP_PROP_CAP);
+  L.prop = prop;
   SelfInfo S;
   self_setup(geo, sd < 0 ? -sd : sd, tn, mk(0.0, 0.0), S);
   double v[24];

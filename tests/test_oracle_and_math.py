@@ -265,3 +265,37 @@ def test_veri_fixture_matches_reference_log():
         assert abs(F[2] - log[f"F{ty}"][1]) <= 5e-14 * abs(F[2])
         # the torque is a small difference of large moments: 12 of its printed digits agree
         assert abs(N[1] - log[f"N{ty}y"]) <= 1e-11 * abs(N[1])
+
+
+def test_ex2_fixture_matches_reference_log():
+    """analysis_sample2/example1.log of the reference (cone_m1 triangles, rotated by pi about x
+    on the solver's command line): total field at (0.3, 0, 1.1) and the radiation force."""
+    g = golden("bv_ex2.npz")
+    assert np.allclose(g["probe/r"][0], [0.3, 0.0, 1.1])
+    log = {  # analysis_sample2/example1.log, lines 34-56
+        "E0": [-5.84203979042922e-02 - 1.71331280017757e-02j, -1.59605270636755e-02 - 5.97684924605190e-03j],
+        "H0": -7.70668013359473e-02 - 1.95100100680507e-02j,
+        "E1": [-5.84233473949296e-02 - 1.71333199922096e-02j, -1.59568962146879e-02 - 5.95361410446437e-03j],
+        "H1": -7.70672750262359e-02 - 1.95107411607629e-02j,
+        "F0": [-2.26647784396326e-04, -1.51648727283879e-05],
+        "F1": [-2.05481609738202e-04, -3.33790381045709e-05],
+    }
+    for ty in (0, 1):
+        E, H = g[f"probe/E{ty}"][0], g[f"probe/H{ty}"][0]
+        assert abs(E[0] - log[f"E{ty}"][0]) <= 5e-14 * abs(E[0])
+        assert abs(E[2] - log[f"E{ty}"][1]) <= 5e-14 * abs(E[2])
+        assert abs(H[1] - log[f"H{ty}"]) <= 5e-14 * abs(H[1])
+        # the force sums singular boundary integrals whose last digits depend on the compiler that
+        # produced the log (the reference's own build here agrees with it to 10 digits)
+        F = g[f"force/F{ty}"]
+        assert abs(F[0] - log[f"F{ty}"][0]) <= 1e-10 * abs(F[0])
+        assert abs(F[2] - log[f"F{ty}"][1]) <= 1e-10 * abs(F[2])
+
+
+def test_rotation_reproduces_result_file_nodes():
+    """Problem's rotation/translation (rotation_translation_obj) gives the node coordinates the
+    reference stored in its result file, bit for bit."""
+    from bem3_emf_qd2_b200.dqd2 import problem_from_arrays
+    g = golden("bv_ex2.npz")
+    p = problem_from_arrays({k[3:]: g[k] for k in g.files if k.startswith("in/")})
+    assert np.array_equal(p.rn[1:], g["dat/rn"][1:])
