@@ -142,36 +142,52 @@ __device__ __forceinline__ void store_pair(const AssembleArgs& A, int row, int s
 #ifndef REGP_MIN_BLOCKS
 #define REGP_MIN_BLOCKS 4  // 4 x 256 threads per SM: 64 registers, 32 warps per SM (measured fastest)
 #endif
-__global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleArgs A, QPLattice L, long long p0, long long np,
-                                                      double3* Fp, unsigned* gh_list, unsigned* gh_count,
-                                                      unsigned gh_cap, int* status)
+// Per-warp pair data in shared memory: the source element and the collocation node with its
+// tangents, read by all lanes.  With them and the lanes' sums in shared memory, only a lane's
+// current quadrature point stays live in registers across the (out-of-line) lattice sums.
+struct RegWarp {
+  Elem es;
+  double rt[3], vtz[3], vte[3];
+};
+
+__global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleArgs A, const __grid_constant__ QPLattice L,
+                                                                       long long p0, long long np, double3* Fp,
+                                                                       unsigned* gh_list, unsigned* gh_count,
+                                                                       unsigned gh_cap, int* status)
 {
+  __shared__ RegWarp sw[8];
+  __shared__ AccP sacc[256];
   long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
-  if (w >= np) return;
+  if (w >= np) return;  // uniform across the warp
   long long p = p0 + w;
   PairIdx q = pair_of(p, A.ne);
-  int tnn;
-  double rt[3], vtz[3], vte[3];
-  target_info(A.geo, A.sid, q.t, q.tn, rt, vtz, vte, tnn);
+  const int at = abs(A.sid[q.t]);
+  const int tnn = (int)A.geo[(size_t)at * GEO_STRIDE + GEO_NN];
   if ((q.tn == 3 && tnn == 3) || q.s == q.t) return;
-  Elem es;
-  load_elem(A.geo, abs(A.sid[q.s]), es);
-  const int npts = (es.nn == 4) ? 144 : 432;
-  AccP a;
+  RegWarp& W = sw[threadIdx.x >> 5];
+  if (lane == 0) {
+    int tn_unused;
+    target_info(A.geo, A.sid, q.t, q.tn, W.rt, W.vtz, W.vte, tn_unused);
+    load_elem(A.geo, abs(A.sid[q.s]), W.es);
+  }
+  AccP& a = sacc[threadIdx.x];
   accp_zero(a);
+  __syncwarp();
+  const int npts = (W.es.nn == 4) ? 144 : 432;
   int err = 0, nterms = 0;
   for (int k = lane; k < npts; k += 32) {
     double z, e, wt;
-    rule_point(es.nn, 12, c_xl, c_wl, k, z, e, wt);
-    int e2 = accp_point(es, L, rt, vtz, vte, z, e, wt, a);
+    rule_point(W.es.nn, 12, c_xl, c_wl, k, z, e, wt);
+    int e2 = accp_point(W.es, L, W.rt, W.vtz, W.vte, z, e, wt, a);
     if (e2 < 0) err = e2;
     else nterms += e2;
   }
   double v[19];
   accp_pack(a, v);
   warp_sum_arr<19>(v);
-  accp_unpack(v, a);
+  AccP s;
+  accp_unpack(v, s);
   err = warp_min_i(err);
   if (lane == 0) record_status(status, err);
   if (A.terms) {
@@ -179,7 +195,7 @@ __global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleA
     if (lane == 0) atomicAdd(A.terms, (unsigned long long)tc);
   }
   cplx CC[9], dCz[9], dCe[9];
-  accp_finish(es, a, CC, dCz, dCe);
+  accp_finish(W.es, s, CC, dCz, dCe);
   if (needs_gh(dCz[8].re, dCe[8].re)) {
     if (lane == 0) {
       unsigned slot = atomicAdd(gh_count, 1u);
@@ -192,7 +208,7 @@ __global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleA
 }
 
 // Near-singular periodic pairs: one CTA (256 threads) per listed pair, 64x64 rule.
-__global__ void __launch_bounds__(256, 1) k_gh_periodic(AssembleArgs A, QPLattice L, long long p0, double3* Fp,
+__global__ void __launch_bounds__(256, 1) k_gh_periodic(AssembleArgs A, const __grid_constant__ QPLattice L, long long p0, double3* Fp,
                                                      const unsigned* gh_list, const unsigned* gh_count, int* status)
 {
   __shared__ double red[8][19];
@@ -351,7 +367,7 @@ __global__ void k_rowsum(AssembleArgs A, int row0, int nrows, const double3* Fp,
 // q0_lit_dcoef_bd_vt2_cc_DV q0_lit_dcoef_v2_cc.c:331-342).  One CTA per (t, tn); the point loop
 // and the combination are self_per_points / self_per_combine (self.cuh).
 #define SELF_THREADS 256
-__global__ void __launch_bounds__(SELF_THREADS, 1) k_self_periodic(AssembleArgs A, QPLattice L, double3* Fself, int* status)
+__global__ void __launch_bounds__(SELF_THREADS, 1) k_self_periodic(AssembleArgs A, const __grid_constant__ QPLattice L, double3* Fself, int* status)
 {
   __shared__ double red[SELF_THREADS / 32][24];
   __shared__ int serr[SELF_THREADS / 32];
@@ -421,6 +437,11 @@ static int ensure_tables(void)
   if (cudaMemcpyToSymbol(c_wl, wl, sizeof wl) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_xh, xh, sizeof xh) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_wh, wh, sizeof wh) != cudaSuccess) return -1;
+  // k_reg_periodic keeps ~40 KB of shared memory per block and runs 4 blocks per SM: ask for the
+  // largest shared-memory carve-out so that the occupancy is not cut by the L1 split
+  if (cudaFuncSetAttribute(k_reg_periodic, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+    return -1;
   if (dev < 64) g_tables_ready[dev] = 1;
   return 0;
 }

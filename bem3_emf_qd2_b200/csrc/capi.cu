@@ -56,11 +56,12 @@ int ensure_scratch(size_t bytes, DevRes** out)
 }
 
 // The lattice's propagating orders into device memory `dst` (QP_PROP_CAP entries) on `st`, for
-// the hoisted spectral sums; without room the sums keep the reference's order (nprop = -1).
+// the hoisted spectral sums of the assembly kernels.
 int attach_prop_list(QPLattice* L, QPProp* dst, cudaStream_t st)
 {
   static thread_local QPProp host[QP_PROP_CAP];
   const int n = qp_prop_list(*L, host, QP_PROP_CAP);
+  if (n < 0) return BEM3_ERR_LATTICE;  // more propagating orders than the list holds
   L->prop = dst;
   L->nprop = n;
   if (n > 0 && cudaMemcpyAsync(dst, host, sizeof(QPProp) * (size_t)n, cudaMemcpyHostToDevice, st) != cudaSuccess)
@@ -79,7 +80,7 @@ int lattice_from(const bem3_qpd2* qd, QPLattice* L)
 }  // namespace
 
 // ------------------------------------------------------------------------------------------
-__global__ void k_qpgf_points(QPLattice L, int n, const double* __restrict__ r, double* __restrict__ out,
+__global__ void k_qpgf_points(const __grid_constant__ QPLattice L, int n, const double* __restrict__ r, double* __restrict__ out,
                               int* __restrict__ ret, int mode)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -174,11 +174,9 @@ BEM_HD void accp_zero(AccP& a)
   a.F = 0; a.dF0 = 0; a.dF1 = 0;
 }
 
-// Adds the contribution of one quadrature point; returns the QPGF status (<0: error).
-BEM_HD int accp_point(const Elem& e, const QPLattice& L, const double* rt, const double* v0, const double* v1,
-                      double zeta, double eta, double w, AccP& a)
+// Source point r(zeta, eta) relative to the target rt, and the Jacobian normal W there.
+BEM_HD void point_geom(const Elem& e, double zeta, double eta, const double* rt, double* vR, double* vW)
 {
-  double vR[3], vW[3];
   if (e.nn == 4) {
     bil_rw(e, zeta, eta, vR, vW);
   } else {
@@ -186,13 +184,25 @@ BEM_HD int accp_point(const Elem& e, const QPLattice& L, const double* rt, const
     vW[0] = e.cw[0][0]; vW[1] = e.cw[1][0]; vW[2] = e.cw[2][0];
   }
   for (int l = 0; l < 3; l++) vR[l] -= rt[l];
+}
+
+// Adds the contribution of one quadrature point; returns the QPGF status (<0: error) or the
+// number of lattice terms.
+BEM_HD int accp_point(const Elem& e, const QPLattice& L, const double* rt, const double* v0, const double* v1,
+                      double zeta, double eta, double w, AccP& a)
+{
+  double vR[3], vW[3];
+  point_geom(e, zeta, eta, rt, vR, vW);
+  QPVal g;
+  int err = qpgf_eval<QP_V1, true>(L, vR, g);
+  // the geometry once more, after the lattice sums: only (zeta, eta, w) stay live across them
+  // (the callers keep the element, the target and the sums in shared memory)
+  point_geom(e, zeta, eta, rt, vR, vW);
   double aR = vnorm3(vR);
   double i_aR = 1.0 / aR;
   double rdW = dot3(vR, vW) * i_aR;
   double rdv0 = dot3(vR, v0) * i_aR, rdv1 = dot3(vR, v1) * i_aR;
   double Wdv0 = dot3(vW, v0), Wdv1 = dot3(vW, v1);
-  QPVal g;
-  int err = qpgf_eval<QP_V1, true>(L, vR, g);
   cplx hn = g.dG[0] * vW[0] + g.dG[1] * vW[1] + g.dG[2] * vW[2];
   double N[4];
   double i3 = i_aR * i_aR * i_aR;

@@ -97,7 +97,7 @@ __device__ __forceinline__ void block_sum_n(double (*red)[FIELD_THREADS], double
   }
 }
 
-__global__ void __launch_bounds__(FIELD_THREADS) k_field(FieldArgs A, QPLattice L, int n, const double* __restrict__ r,
+__global__ void __launch_bounds__(FIELD_THREADS) k_field(FieldArgs A, const __grid_constant__ QPLattice L, int n, const double* __restrict__ r,
                                                         const int* __restrict__ did, const int2* __restrict__ cell,
                                                         int type, int total, double* __restrict__ Eo,
                                                         double* __restrict__ Ho, int* status)

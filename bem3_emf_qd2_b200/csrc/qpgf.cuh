@@ -90,6 +90,19 @@ extern unsigned long long bem_stat_t[5];  // real-space, spectral prop., spectra
 #define BEM_STAT_T(i) ((void)0)
 #endif
 
+// Special functions of the terms, out of line when QP_SPECIAL_NOINLINE is set (one copy of their
+// code for all call sites).
+#if defined(QP_SPECIAL_NOINLINE)
+BEM_HD_NOINLINE double qp_erfc(double x) { return erfc(x); }
+#else
+BEM_HD double qp_erfc(double x) { return erfc(x); }
+#endif
+#if defined(QP_EXP_NOINLINE)
+BEM_HD_NOINLINE double qp_exp(double x) { return exp(x); }
+#else
+BEM_HD double qp_exp(double x) { return exp(x); }
+#endif
+
 // ---------------------------------------------------------------------------------------------
 // Ewald real-space term (d3_qpgf_d2.c:1814-1838).  F and dF[3] (dF[2] still lacks the
 // factor -z/(4 pi) that the sum applies at the end).  ce = e^{i k||.R_l} is supplied by the
@@ -113,7 +126,7 @@ BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1
   double ke = L.k * veps;
   double i_ve = 1.0 / veps;
   double rl_2e = rl * 0.5 * i_ve;
-  double ef = exp(ke * ke - rl_2e * rl_2e);
+  double ef = qp_exp(ke * ke - rl_2e * rl_2e);
   cplx w = faddeeva_w_t<FAST>(ke, rl_2e);
   double cfr = i_rl * i_rl * ef * (i_rl * w.re - L.k * w.im + i_ve * QP_INV_SQRTPI);
   cplx cf = ce * cfr;
@@ -147,9 +160,16 @@ BEM_HD void qp_ew2_evan(const double* r, double veps, double an0, double an1, do
 {
   BEM_STAT_T(2);
   double azve = r[2] / (2.0 * veps);
-  double ebz = exp(bn * r[2]);
-  double f1 = ebz * erfc(bn * veps + azve);
-  double f2 = 1.0 / ebz * erfc(bn * veps - azve);
+  double ebz = qp_exp(bn * r[2]);
+  // both erfc values from one call site (one copy of its code in the sums)
+  double e1 = 0.0, e2 = 0.0;
+#pragma unroll 1
+  for (int j = 0; j < 2; j++) {
+    const double v = qp_erfc(j == 0 ? bn * veps + azve : bn * veps - azve);
+    if (j == 0) e1 = v; else e2 = v;
+  }
+  double f1 = ebz * e1;
+  double f2 = 1.0 / ebz * e2;
   // Fn = ce / (i bn) (f1 + f2) = -i ce (f1+f2)/bn
   F = mul_mi(ce * ((f1 + f2) * ibn));
   dF[0] = F * an0;
@@ -186,7 +206,7 @@ BEM_HD void qp_fd_prop(const double* r, double an0, double an1, double bn, cplx 
 BEM_HD void qp_fd_evan(const double* r, double an0, double an1, double bn, double ibn, cplx ph, cplx& F, cplx* dF)
 {
   BEM_STAT_T(4);
-  dF[2] = ph * exp(-bn * fabs(r[2]));
+  dF[2] = ph * qp_exp(-bn * fabs(r[2]));
   F = mul_mi(dF[2] * ibn);
   dF[0] = F * an0;
   dF[1] = F * an1;
@@ -302,8 +322,8 @@ QP_SUM_FN int qp_ew1_sum(const QPLattice& L, const double* r, double veps, doubl
 // passes over the propagating positions (they still count for the row rule).  The stop rules see
 // the propagating contributions earlier than the reference's order, so a sum may stop a term
 // sooner or later; every neglected term is still below the rule's relative threshold (1e-16 of
-// the running sum).  Without a list (L.nprop < 0) the sum runs in the reference's order.  OPT
-// also selects the division-light w(z) (faddeeva_w_t<true>).
+// the running sum).  OPT callers must attach the list (qp_prop_list); OPT also selects the
+// division-light w(z) (faddeeva_w_t<true>).
 template <int MODE, int FD, bool OPT = false>
 QP_SUM_FN int qp_spec_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
 {
@@ -311,7 +331,7 @@ QP_SUM_FN int qp_spec_sum(const QPLattice& L, const double* r, double veps, doub
   const int LIMIT = FD ? QP_FD_LIMIT : QP_EW_LIMIT;
   const int ELIM = FD ? -1 : -2;
   S = mk(0, 0); dS[0] = mk(0, 0); dS[1] = mk(0, 0); dS[2] = mk(0, 0);
-  const bool hoist = OPT && L.nprop >= 0;
+  const bool hoist = OPT;  // OPT callers always attach the list (L.nprop >= 0)
   int cc = 0;
   if (hoist) {
 #pragma unroll 1

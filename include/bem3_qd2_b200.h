@@ -23,7 +23,7 @@ extern "C" {
 #define BEM3_ERR_ARG -1      /* invalid argument */
 #define BEM3_ERR_CUDA -2     /* CUDA failure (device memory, launch, copy) */
 #define BEM3_ERR_SCRATCH -3  /* scratch smaller than required */
-#define BEM3_ERR_LATTICE -4  /* degenerate lattice, det[d1 d2] == 0 */
+#define BEM3_ERR_LATTICE -4  /* degenerate lattice (det[d1 d2] == 0) or more than 2048 propagating orders */
 #define BEM3_ERR_SOLVE -5    /* singular system */
 /* Kernel status codes (returned as is): -11..-14 and -21..-24 are the QPGF failures of
  * d3hm_qpgf_d2_v1 (qgf2_src/d3_qpgf_d2.h:112-123); -900 near-singular work-list overflow. */
