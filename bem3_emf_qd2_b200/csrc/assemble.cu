@@ -138,9 +138,8 @@ __device__ __forceinline__ void store_pair(const AssembleArgs& A, int row, int s
 }
 
 // ==========================================================================================
-// Regular periodic pairs: one warp per pair.
 #ifndef REGP_MIN_BLOCKS
-#define REGP_MIN_BLOCKS 4  // 4 x 256 threads per SM: 64 registers, 32 warps per SM (measured fastest)
+#define REGP_MIN_BLOCKS 2  // 2 x 256 threads per SM: 128 registers (measured fastest with register-resident sums)
 #endif
 // Per-warp pair data in shared memory: the source element and the collocation node with its
 // tangents, read by all lanes.  With them and the lanes' sums in shared memory, only a lane's
@@ -149,62 +148,83 @@ struct RegWarp {
   Elem es;
   double rt[3], vtz[3], vte[3];
 };
+#define REGP_PAIRS 2  // pairs per warp: 2 x 144 Gauss points = 9 per lane, no ragged last step
+#define REGP_SMEM_BYTES (sizeof(RegWarp) * 8 * REGP_PAIRS + sizeof(AccP) * 256 * REGP_PAIRS)
 
+// Regular periodic pairs: one warp per REGP_PAIRS consecutive pairs of the chunk; lane l takes the
+// points l, l + 32, ... of the pairs' concatenated point lists.
 __global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleArgs A, const __grid_constant__ QPLattice L,
                                                                        long long p0, long long np, double3* Fp,
                                                                        unsigned* gh_list, unsigned* gh_count,
                                                                        unsigned gh_cap, int* status)
 {
-  __shared__ RegWarp sw[8];
-  __shared__ AccP sacc[256];
-  long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (w >= np) return;  // uniform across the warp
-  long long p = p0 + w;
-  PairIdx q = pair_of(p, A.ne);
-  const int at = abs(A.sid[q.t]);
-  const int tnn = (int)A.geo[(size_t)at * GEO_STRIDE + GEO_NN];
-  if ((q.tn == 3 && tnn == 3) || q.s == q.t) return;
-  RegWarp& W = sw[threadIdx.x >> 5];
-  if (lane == 0) {
-    int tn_unused;
-    target_info(A.geo, A.sid, q.t, q.tn, W.rt, W.vtz, W.vte, tn_unused);
-    load_elem(A.geo, abs(A.sid[q.s]), W.es);
+  extern __shared__ __align__(16) unsigned char regp_smem[];  // REGP_SMEM_BYTES
+  RegWarp(*sw)[REGP_PAIRS] = reinterpret_cast<RegWarp(*)[REGP_PAIRS]>(regp_smem);
+  AccP(*sacc)[256] = reinterpret_cast<AccP(*)[256]>(regp_smem + sizeof(RegWarp) * 8 * REGP_PAIRS);
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const long long first = w * REGP_PAIRS;  // pair index within the chunk
+  if (first >= np) return;  // uniform across the warp
+  int npts[REGP_PAIRS];
+  PairIdx q[REGP_PAIRS];
+#pragma unroll
+  for (int j = 0; j < REGP_PAIRS; j++) {
+    npts[j] = 0;
+    if (first + j >= np) continue;
+    q[j] = pair_of(p0 + first + j, A.ne);
+    const int at = abs(A.sid[q[j].t]);
+    const int tnn = (int)A.geo[(size_t)at * GEO_STRIDE + GEO_NN];
+    if ((q[j].tn == 3 && tnn == 3) || q[j].s == q[j].t) continue;
+    RegWarp& W = sw[wib][j];
+    if (lane == 0) {
+      int tn_unused;
+      target_info(A.geo, A.sid, q[j].t, q[j].tn, W.rt, W.vtz, W.vte, tn_unused);
+      load_elem(A.geo, abs(A.sid[q[j].s]), W.es);
+    }
+    const int sn = (int)A.geo[(size_t)abs(A.sid[q[j].s]) * GEO_STRIDE + GEO_NN];
+    npts[j] = (sn == 4) ? 144 : 432;
+    accp_zero(sacc[j][threadIdx.x]);
   }
-  AccP& a = sacc[threadIdx.x];
-  accp_zero(a);
   __syncwarp();
-  const int npts = (W.es.nn == 4) ? 144 : 432;
+  const int ntot = npts[0] + (REGP_PAIRS > 1 ? npts[1] : 0);
   int err = 0, nterms = 0;
-  for (int k = lane; k < npts; k += 32) {
+  for (int k = lane; k < ntot; k += 32) {
+    const int j = (k < npts[0]) ? 0 : 1;
+    const int kk = j ? k - npts[0] : k;
+    const RegWarp& W = sw[wib][j];
     double z, e, wt;
-    rule_point(W.es.nn, 12, c_xl, c_wl, k, z, e, wt);
-    int e2 = accp_point(W.es, L, W.rt, W.vtz, W.vte, z, e, wt, a);
+    rule_point(W.es.nn, 12, c_xl, c_wl, kk, z, e, wt);
+    int e2 = accp_point(W.es, L, W.rt, W.vtz, W.vte, z, e, wt, sacc[j][threadIdx.x]);
     if (e2 < 0) err = e2;
     else nterms += e2;
   }
-  double v[19];
-  accp_pack(a, v);
-  warp_sum_arr<19>(v);
-  AccP s;
-  accp_unpack(v, s);
   err = warp_min_i(err);
   if (lane == 0) record_status(status, err);
   if (A.terms) {
     double tc = warp_sum((double)nterms);
     if (lane == 0) atomicAdd(A.terms, (unsigned long long)tc);
   }
-  cplx CC[9], dCz[9], dCe[9];
-  accp_finish(W.es, s, CC, dCz, dCe);
-  if (needs_gh(dCz[8].re, dCe[8].re)) {
-    if (lane == 0) {
-      unsigned slot = atomicAdd(gh_count, 1u);
-      if (slot < gh_cap) gh_list[slot] = (unsigned)w;
-      else record_status(status, -900);
+#pragma unroll 1
+  for (int j = 0; j < REGP_PAIRS; j++) {
+    if (npts[j] == 0) continue;  // uniform across the warp
+    double v[19];
+    accp_pack(sacc[j][threadIdx.x], v);
+    warp_sum_arr<19>(v);
+    AccP s;
+    accp_unpack(v, s);
+    cplx CC[9], dCz[9], dCe[9];
+    accp_finish(sw[wib][j].es, s, CC, dCz, dCe);
+    const long long pi = first + j;
+    if (needs_gh(dCz[8].re, dCe[8].re)) {
+      if (lane == 0) {
+        unsigned slot = atomicAdd(gh_count, 1u);
+        if (slot < gh_cap) gh_list[slot] = (unsigned)pi;
+        else record_status(status, -900);
+      }
+      continue;
     }
-    return;
+    store_pair(A, q[j].row, q[j].s, CC, dCz, dCe, Fp, pi, lane);
   }
-  store_pair(A, q.row, q.s, CC, dCz, dCe, Fp, w, lane);
 }
 
 // Near-singular periodic pairs: one CTA (256 threads) per listed pair, 64x64 rule.
@@ -437,10 +457,12 @@ static int ensure_tables(void)
   if (cudaMemcpyToSymbol(c_wl, wl, sizeof wl) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_xh, xh, sizeof xh) != cudaSuccess) return -1;
   if (cudaMemcpyToSymbol(c_wh, wh, sizeof wh) != cudaSuccess) return -1;
-  // k_reg_periodic keeps ~40 KB of shared memory per block and runs 4 blocks per SM: ask for the
-  // largest shared-memory carve-out so that the occupancy is not cut by the L1 split
+  // k_reg_periodic keeps ~80 KB of shared memory per block (dynamic, above the 48 KB static
+  // limit): allow it, and ask for the largest carve-out so the L1 split does not cut occupancy
   if (cudaFuncSetAttribute(k_reg_periodic, cudaFuncAttributePreferredSharedMemoryCarveout,
-                           (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+                           (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess ||
+      cudaFuncSetAttribute(k_reg_periodic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)REGP_SMEM_BYTES) !=
+          cudaSuccess)
     return -1;
   if (dev < 64) g_tables_ready[dev] = 1;
   return 0;
@@ -499,10 +521,10 @@ int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, 
     long long p0 = (long long)r0 * ne, np = (long long)nr * ne;
     cudaMemsetAsync(gh_count, 0, sizeof(unsigned), st);
     if (A.periodic) {
-      long long threads = np * 32;
+      long long threads = (np + REGP_PAIRS - 1) / REGP_PAIRS * 32;
       unsigned blocks = (unsigned)((threads + 255) / 256);
       if (timing) cudaEventRecord(ev0, st);
-      k_reg_periodic<<<blocks, 256, 0, st>>>(A, *L, p0, np, Fp, gh_list, gh_count, gh_cap, d_status);
+      k_reg_periodic<<<blocks, 256, REGP_SMEM_BYTES, st>>>(A, *L, p0, np, Fp, gh_list, gh_count, gh_cap, d_status);
       if (timing) {
         cudaEventRecord(ev1, st);
         cudaEventSynchronize(ev1);

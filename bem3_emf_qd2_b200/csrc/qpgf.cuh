@@ -253,7 +253,7 @@ BEM_HD int qp_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx 
 #endif
 
 template <int MODE, bool OPT = false>
-QP_SUM_FN int qp_ew1_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
+BEM_HD int qp_ew1_sum_body(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
 {
   S = mk(0, 0); dS[0] = mk(0, 0); dS[1] = mk(0, 0); dS[2] = mk(0, 0);
   cplx oS = S, od0 = S, od1 = S;
@@ -325,7 +325,7 @@ QP_SUM_FN int qp_ew1_sum(const QPLattice& L, const double* r, double veps, doubl
 // the running sum).  OPT callers must attach the list (qp_prop_list); OPT also selects the
 // division-light w(z) (faddeeva_w_t<true>).
 template <int MODE, int FD, bool OPT = false>
-QP_SUM_FN int qp_spec_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
+BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS)
 {
   if (FD && r[2] == 0.0) return -4;
   const int LIMIT = FD ? QP_FD_LIMIT : QP_EW_LIMIT;
@@ -445,6 +445,27 @@ QP_SUM_FN int qp_spec_sum(const QPLattice& L, const double* r, double veps, doub
     dS[2] = dS[2] * (0.25 * aidd);
   }
   return cc;
+}
+
+// The sums as called: the point and the running sums are copied into locals so that, out of line,
+// they live in registers (through the caller's pointers every term would read and write memory).
+template <int MODE, bool OPT = false>
+QP_SUM_FN int qp_ew1_sum(const QPLattice& L, const double* r_in, double veps, double eps, cplx& S_out, cplx* dS_out)
+{
+  const double r[3] = {r_in[0], r_in[1], r_in[2]};
+  cplx S, dS[3];
+  const int ret = qp_ew1_sum_body<MODE, OPT>(L, r, veps, eps, S, dS);
+  S_out = S; dS_out[0] = dS[0]; dS_out[1] = dS[1]; dS_out[2] = dS[2];
+  return ret;
+}
+template <int MODE, int FD, bool OPT = false>
+QP_SUM_FN int qp_spec_sum(const QPLattice& L, const double* r_in, double veps, double eps, cplx& S_out, cplx* dS_out)
+{
+  const double r[3] = {r_in[0], r_in[1], r_in[2]};
+  cplx S, dS[3];
+  const int ret = qp_spec_sum_body<MODE, FD, OPT>(L, r, veps, eps, S, dS);
+  S_out = S; dS_out[0] = dS[0]; dS_out[1] = dS[1]; dS_out[2] = dS[2];
+  return ret;
 }
 
 // ---------------------------------------------------------------------------------------------
