@@ -107,6 +107,7 @@ def lib():
         L.bem3_ctx_set_bv.argtypes = [vp, C.POINTER(bem3_bv)]
         L.bem3_ctx_domain_id.argtypes = [vp, i, vp, vp]
         L.bem3_ctx_field.argtypes = [vp, i, vp, i, i, vp, vp, vp]
+        L.bem3_ctx_force.argtypes = [vp, vp, i, vp, vp]
         L.bem3_geo_stride.restype = i
         L.bem3_last_gh_pairs.restype = C.c_ulonglong
         L.bem3_gauss_legendre.argtypes = [i, vp, vp]
@@ -281,6 +282,14 @@ class Context:
         did = np.zeros(len(r), np.int32)
         check(lib().bem3_ctx_domain_id(self.h, len(r), _ptr(r), _ptr(did)), "bem3_ctx_domain_id")
         return did
+
+    def force(self, rc=(0.0, 0.0, 0.0), type_: int = 0):
+        """Radiation force F[3] and torque N[3] about rc (force_FN)."""
+        rc = np.ascontiguousarray(rc, dtype=np.float64)
+        F = np.zeros(3)
+        N = np.zeros(3)
+        check(lib().bem3_ctx_force(self.h, _ptr(rc), type_, _ptr(F), _ptr(N)), "bem3_ctx_force")
+        return F, N
 
     def field(self, r, type_: int = 0, total: bool = True):
         """E, H [n,3] complex and the domain of each point (EH_t if total else EH_s)."""

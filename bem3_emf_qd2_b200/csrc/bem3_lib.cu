@@ -5,5 +5,6 @@
 #include "capi.cu"
 #include "solve.cu"
 #include "field.cu"
+#include "force.cu"
 #include "solve_dtn.cu"
 #include "context.cu"

@@ -19,6 +19,7 @@ struct bem3_ctx_s {
   DevBuf dsid[BEM3_MAXDOM];
   DevBuf U[BEM3_MAXDOM], dU[BEM3_MAXDOM], E[BEM3_MAXDOM], H[BEM3_MAXDOM], dE[BEM3_MAXDOM], dH[BEM3_MAXDOM];
   DevBuf status;
+  DevBuf prop;  // the lattice's propagating orders (the optimised lattice sums of the self rule)
 };
 
 namespace {
@@ -67,9 +68,17 @@ extern "C" int bem3_ctx_create(const bem3_problem* P, bem3_ctx* out)
   c->lambda0 = P->lambda0;
   c->qd = P->qd;
   memset(&c->L, 0, sizeof c->L);
-  if (P->ps == 1 && qp_lattice_init(c->L, P->qd.k, P->qd.vk[0], P->qd.vk[1], P->qd.vd1[0], P->qd.vd1[1], P->qd.vd2[0],
-                                    P->qd.vd2[1]) != 0)
-    return fail(BEM3_ERR_LATTICE);
+  if (P->ps == 1) {
+    if (qp_lattice_init(c->L, P->qd.k, P->qd.vk[0], P->qd.vk[1], P->qd.vd1[0], P->qd.vd1[1], P->qd.vd2[0],
+                        P->qd.vd2[1]) != 0)
+      return fail(BEM3_ERR_LATTICE);
+    std::vector<QPProp> pl(QP_PROP_CAP);
+    const int np = qp_prop_list(c->L, pl.data(), QP_PROP_CAP);
+    if (np < 0) return fail(BEM3_ERR_LATTICE);
+    if ((rc = upload(c->prop, pl.data(), (size_t)(np > 0 ? np : 1)))) return fail(rc);
+    c->L.prop = c->prop.as<QPProp>();
+    c->L.nprop = np;
+  }
   const int Ne = P->Ne, MN = P->MN;
   c->nv.assign(P->mesh.nv, P->mesh.nv + Ne + 1);
   c->eni_h.assign(P->eni, P->eni + 4 * (size_t)(Ne + 1));
@@ -521,6 +530,42 @@ extern "C" int bem3_ctx_field(bem3_ctx c, int n, const double* r, int type, int 
       cudaMemcpy(H, dH.p, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
       (did && cudaMemcpy(did, ddid.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess))
     return BEM3_ERR_CUDA;
+  return hs;
+}
+
+extern "C" int bem3_ctx_force(bem3_ctx c, const double* rc, int type, double* F, double* N)
+{
+  if (!c || !rc || !F || !N || (type != 0 && type != 1)) return BEM3_ERR_ARG;
+  DeviceGuard g(c->dev);
+  const int ne = (int)c->sid[0].size();
+  // the boundary field at points other than nodes needs the periodic self rule
+  bool needs_bd = (type == 1);
+  for (int s : c->sid[0]) needs_bd = needs_bd || (c->nv[abs(s)] == 3);
+  if (needs_bd && c->ps != 1) return BEM3_ERR_ARG;
+  if (ensure_tables() != 0) return BEM3_ERR_CUDA;
+  ForceArgs A;
+  memset(&A, 0, sizeof A);
+  A.geo = c->geo.as<double>(); A.ne = ne; A.sid = c->dsid[0].as<int>();
+  A.E = c->E[0].as<double>(); A.dE = c->dE[0].as<double>(); A.H = c->H[0].as<double>(); A.dH = c->dH[0].as<double>();
+  A.k0re = c->kn[0]; A.k0im = c->kn[1];
+  const double n0 = c->kn[0] * c->lambda0 / (2.0 * QP_PI);  // kn[0] = 2 pi n0 / lambda0
+  A.epd = n0 * n0;
+  for (int l = 0; l < 3; l++) A.rc[l] = rc[l];
+  A.type = type;
+  A.waves = c->waves.as<bem3_wave>(); A.nwaves = c->nwaves;
+  const int npt = ne * FORCE_MAXPTS;
+  DevBuf part, res;
+  if (part.alloc((size_t)npt * 6 * sizeof(double)) || res.alloc(6 * sizeof(double))) return BEM3_ERR_CUDA;
+  cudaMemset(c->status.p, 0, sizeof(int));
+  k_force_points<<<npt, FORCE_THREADS>>>(A, c->L, part.as<double>(), c->status.as<int>());
+  k_force_sum<<<1, FORCE_THREADS>>>(part.as<double>(), npt, res.as<double>());
+  if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
+  double h[6];
+  int hs = 0;
+  if (cudaMemcpy(h, res.p, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(&hs, c->status.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return BEM3_ERR_CUDA;
+  for (int l = 0; l < 3; l++) { F[l] = h[l]; N[l] = h[3 + l]; }
   return hs;
 }
 

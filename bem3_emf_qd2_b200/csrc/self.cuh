@@ -34,6 +34,23 @@ struct SelfInfo {
   double Tz[3], Te[3];  // unnormalised tangents at the node
 };
 
+// Self integral around the point (zt, et) of element aid (collocation nodes use their own
+// parameters; the boundary field of the force evaluation uses other points of the element).
+BEM_HD void self_setup_at(const double* geo, int aid, double zt, double et, cplx k, SelfInfo& S)
+{
+  load_elem(geo, aid, S.e);
+  S.k = k;
+  S.zt = zt;
+  S.et = et;
+  polar_setup(S.e.nn, S.zt, S.et, S.P);
+  S.bil = (S.e.nn == 4);
+  S.curved = S.bil ? !bil_is_plane(S.e) : 0;
+  for (int i = 0; i < 3; i++) {
+    S.Tz[i] = S.e.cr[i][1] + S.e.cr[i][3] * S.et;
+    S.Te[i] = S.e.cr[i][2] + S.e.cr[i][3] * S.zt;
+  }
+}
+
 BEM_HD void self_setup(const double* geo, int aid, int tn, cplx k, SelfInfo& S)
 {
   load_elem(geo, aid, S.e);
@@ -323,8 +340,10 @@ BEM_HD void self_int_combine(const SelfInfo& S, const double* R1, const double* 
 // Layout: G[4] 0..7, H[4] 8..15 (polar rule with the quasi-periodic Green's function), then the
 // free-space solid angle of a curved quad at the node and at its four finite-difference
 // neighbours (zeta +- h, eta +- h): 16..20.  Returns the first QPGF failure code (0 if none).
+// nf: how many solid-angle centres to evaluate (5 for the derivatives of the assembly, 1 when
+// only F at the point is needed).
 BEM_HD int self_per_points(const SelfInfo& S, const QPLattice& L, const double* xl, const double* wl, const double* xh,
-                           const double* wh, int lane, int nlanes, double* v)
+                           const double* wh, int lane, int nlanes, double* v, int nf = 5)
 {
   int err = 0;
   const Elem& e = S.e;
@@ -357,7 +376,7 @@ BEM_HD int self_per_points(const SelfInfo& S, const QPLattice& L, const double* 
     const double h = EL_CDFH;
     const double cz[5] = {S.zt, S.zt + h, S.zt - h, S.zt, S.zt};
     const double ce[5] = {S.et, S.et, S.et, S.et + h, S.et - h};
-    for (int c = 0; c < 5; c++) v[16 + c] += bil_self_F(e, cz[c], ce[c], xl, wl, xh, wh, lane, nlanes);
+    for (int c = 0; c < nf; c++) v[16 + c] += bil_self_F(e, cz[c], ce[c], xl, wl, xh, wh, lane, nlanes);
   }
   return err;
 }

@@ -211,6 +211,13 @@ int bem3_ctx_domain_id(bem3_ctx c, int n, const double *r, int *did);
  * Points outside every domain get did = -1 and zero fields. */
 int bem3_ctx_field(bem3_ctx c, int n, const double *r, int type, int total, double *E, double *H, int *did);
 
+/* Radiation force F[3] and torque N[3] about rc[3] on the objects, from the Maxwell stress tensor
+ * of the total field on the open region's boundary (force_FN, d3qd2_src/d3qd2_force.c:10-54).
+ * type 0: element nodes (plus the centroid on triangles); type 1: 9-point (quads) / 7-point
+ * (triangles) rules, with the boundary field EH_t_bd (d3qd2_field.c:343-385) at the points.
+ * Points other than nodes need the quasi-periodic open region (BEM3_ERR_ARG otherwise). */
+int bem3_ctx_force(bem3_ctx c, const double *rc, int type, double *F, double *N);
+
 /* Gauss-Legendre nodes and weights on [-1, 1] (the reference's gauleg, com_src/gauleg.c:3). */
 void bem3_gauss_legendre(int n, double *x, double *w);
 
