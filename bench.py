@@ -35,8 +35,11 @@ UNIT = "pairs/s"
 # FP64 instructions ncu counts in one launch (2 DFMA + DADD + DMUL, thread level) divided by the
 # terms the kernel's own counter reports for that launch, captured on the workload's /stride8
 # subsample (same lattice, wavelength and element size).  The live roofline figure is
-# terms/s x this number; the captures are summarised in profiles/.
-FP64_OPS_PER_TERM = {}
+# terms/s x this number.
+FP64_OPS_PER_TERM = {"twolayer3072": 273.1}
+# DRAM bytes (read + write) of one k_reg_periodic launch, from the same capture scaled by the
+# pairs processed (64x for stride 8).
+TRAFFIC_PER_LAUNCH = {"twolayer3072": 1.6167e9 * 64}
 
 
 def parse():
@@ -267,7 +270,8 @@ def run_ours(args):
         if ops:
             achieved = terms_per_launch * ops / (per_launch_ms * 1e-3) / 1e12
             roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": None,
+                    "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH.get(args.config),
+                    "fp64_ops_per_term": ops,
                     "kernel": "k_reg_periodic", "peak_source": "measured DFMA probe on this GPU"}
         else:
             roof = {"bound": "fp64", "achieved": None, "peak": peak, "unit": "TFLOP/s", "frac": None,
