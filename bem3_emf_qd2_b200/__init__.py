@@ -103,6 +103,11 @@ def lib():
         L.bem3_ctx_destroy.restype = None
         L.bem3_ctx_solve.argtypes = [vp]
         L.bem3_ctx_set_solver.argtypes = [vp, i]
+        L.bem3_ctx_set_incident.argtypes = [vp, i, vp, vp, vp, vp, vp]
+        L.bem3_ctx_resolve.argtypes = [vp]
+        L.bem3_ctx_release.argtypes = [vp]
+        L.bem3_ctx_device_bytes.argtypes = [vp]
+        L.bem3_ctx_device_bytes.restype = C.c_size_t
         L.bem3_ctx_get_bv.argtypes = [vp, C.POINTER(bem3_bv)]
         L.bem3_ctx_set_bv.argtypes = [vp, C.POINTER(bem3_bv)]
         L.bem3_ctx_domain_id.argtypes = [vp, i, vp, vp]
@@ -262,6 +267,25 @@ class Context:
         """method 0: reduced 4 NN system where applicable, 1: the full 8 NN system, 2: reduced only."""
         check(lib().bem3_ctx_set_solver(self.h, method), "bem3_ctx_set_solver")
         check(lib().bem3_ctx_solve(self.h), "bem3_ctx_solve")
+
+    def set_incident(self, waves) -> None:
+        """Replace the incident plane waves (same wavelength and direction as the solved ones; the
+        matrices and factorisations stay valid) -- bem3_ctx_set_incident."""
+        q = self.p.with_waves(waves)
+        pa = ProblemArrays(q)
+        check(lib().bem3_ctx_set_incident(self.h, len(q.waves), C.cast(pa.waves, C.c_void_p), _ptr(pa.Ui),
+                                          _ptr(pa.dUi), _ptr(pa.dEiz), _ptr(pa.dEie)), "bem3_ctx_set_incident")
+        self.p = q
+
+    def resolve(self) -> None:
+        """Boundary values for the current incident field with the resident factorisations."""
+        check(lib().bem3_ctx_resolve(self.h), "bem3_ctx_resolve")
+
+    def release(self) -> None:
+        check(lib().bem3_ctx_release(self.h), "bem3_ctx_release")
+
+    def device_bytes(self) -> int:
+        return int(lib().bem3_ctx_device_bytes(self.h))
 
     def boundary_values(self):
         out, bvs = _bv_arrays(self.p)

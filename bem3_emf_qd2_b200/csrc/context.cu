@@ -3,6 +3,22 @@
 #include <math.h>
 #include <stdlib.h>
 
+// What a solve leaves on the device so that a new incident field needs only right-hand sides:
+// the matrices of every domain, each domain's compacted G factorised, and the factorised system
+// of the potentials (reduced or full).
+struct SolveState {
+  int method = 0;  // factors held: 0 none, 1 the full 8 NN system, 2 the reduced 4 NN system
+  DevBuf G[BEM3_MAXDOM], H[BEM3_MAXDOM], dG[BEM3_MAXDOM], dH[BEM3_MAXDOM], dF[BEM3_MAXDOM];
+  int n[BEM3_MAXDOM] = {};                 // element nodes of each domain
+  DevBuf gnode[BEM3_MAXDOM], cmap[BEM3_MAXDOM];
+  DevBuf Gc[BEM3_MAXDOM], Gpiv[BEM3_MAXDOM];  // compacted G_d, LU-factorised (column-major)
+  std::vector<int> elim;                   // reduced form: eliminated domains
+  DevBuf nodes;                            // DtnNode[NN]
+  DevBuf K[BEM3_MAXDOM];                   // K_d = G_d^-1 H_d of the eliminated domains
+  DevBuf A, Apiv;                          // the factorised system of the potentials
+  size_t bytes = 0;                        // device memory held
+};
+
 struct bem3_ctx_s {
   int dev = 0;
   int MN = 0, Ne = 0, NN = 0, Nn = 0, ps = 0, nwaves = 0;
@@ -20,6 +36,8 @@ struct bem3_ctx_s {
   DevBuf U[BEM3_MAXDOM], dU[BEM3_MAXDOM], E[BEM3_MAXDOM], H[BEM3_MAXDOM], dE[BEM3_MAXDOM], dH[BEM3_MAXDOM];
   DevBuf status;
   DevBuf prop;  // the lattice's propagating orders (the optimised lattice sums of the self rule)
+  SolveState* st = nullptr;
+  ~bem3_ctx_s() { delete st; }
 };
 
 namespace {
@@ -253,119 +271,258 @@ bool colour_domains(bem3_ctx c, std::vector<int>& elim)
   return true;
 }
 
-// Reduced solve; fills X (device, 8 NN: U then dU, component-major, global node order).
-// Returns 0, 1 when the domain graph does not allow it, or an error code.
-int dtn_solve(bem3_ctx c, SolveDev& S, double* X)
+struct Handles {
+  cusolverDnHandle_t s = nullptr;
+  cublasHandle_t b = nullptr;
+  int init()
+  {
+    if (cusolverDnCreate(&s) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
+    if (cublasCreate(&b) != CUBLAS_STATUS_SUCCESS) return BEM3_ERR_CUDA;
+    return 0;
+  }
+  ~Handles()
+  {
+    if (b) cublasDestroy(b);
+    if (s) cusolverDnDestroy(s);
+  }
+};
+
+DtnArgs dtn_view(bem3_ctx c, const SolveState& T, const SolveDev& S)
 {
-  const int MN = c->MN, NN = c->NN;
-  std::vector<int> elim;
-  if (!colour_domains(c, elim)) return 1;
-  std::vector<DtnNode> nodes((size_t)NN);
-  std::vector<int> seen((size_t)NN, 0);
-  std::vector<std::vector<int>> gnode(MN + 1), cmap(MN + 1);
+  DtnArgs A;
+  A.node = T.nodes.p ? (const DtnNode*)T.nodes.p : nullptr;
+  A.geo = S.geo; A.md = S.md; A.sd = S.sd; A.kn = S.kn; A.NN = c->NN;
+  return A;
+}
+
+SolveDev solve_view_with(bem3_ctx c, SolveState& T)
+{
+  SolveDev S = solve_view(c);
+  for (int d = 0; d <= c->MN; d++) {
+    S.G[d] = T.G[d].as<double>(); S.H[d] = T.H[d].as<double>();
+    S.dG[d] = T.dG[d].as<double>(); S.dH[d] = T.dH[d].as<double>(); S.dF[d] = T.dF[d].as<double>();
+  }
+  return S;
+}
+
+// Phase 1: the coefficient matrices of every domain and the node tables.
+int phase_assemble(bem3_ctx c, SolveState& T)
+{
+  const int MN = c->MN;
+  int rc;
   for (int d = 0; d <= MN; d++) {
-    for (int t = 0; t < S.ne[d]; t++) {
+    const int ne = (int)c->sid[d].size();
+    const size_t N = (size_t)4 * ne;
+    if (T.G[d].alloc(N * N * 16) || T.H[d].alloc(N * N * 16) || T.dG[d].alloc(2 * N * N * 16) ||
+        T.dH[d].alloc(2 * N * N * 16) || T.dF[d].alloc(N * 3 * 8))
+      return BEM3_ERR_CUDA;
+    T.bytes += N * N * 16 * 6 + N * 24;
+    const int periodic = (d == 0 && c->ps == 1) ? 1 : 0;
+    rc = bem3_assemble_domain_dev(c->geo.as<double>(), c->Ne, c->dsid[d].as<int>(), ne, d, periodic, &c->qd,
+                                  c->kn[2 * d], c->kn[2 * d + 1], T.G[d].as<double>(), T.H[d].as<double>(),
+                                  T.dG[d].as<double>(), T.dH[d].as<double>(), T.dF[d].as<double>(), nullptr);
+    if (rc) return rc;
+    std::vector<int> gn, cm;
+    for (int t = 0; t < ne; t++) {
       const int a = abs(c->sid[d][t]);
       for (int tn = 0; tn < c->nv[a]; tn++) {
-        const int g = c->eni_h[4 * a + tn];
-        if (g < 0 || g >= NN) return BEM3_ERR_ARG;
-        const int j = (int)gnode[d].size();
-        gnode[d].push_back(g);
-        cmap[d].push_back(4 * t + tn);
-        DtnNode& q = nodes[g];
-        q.elem = a; q.l = tn;
-        if (elim[d]) { q.de = d; q.le = j; seen[g] |= 1; }
-        else { q.dn = d; q.ln = j; seen[g] |= 2; }
+        gn.push_back(c->eni_h[4 * a + tn]);
+        cm.push_back(4 * t + tn);
       }
     }
+    T.n[d] = (int)gn.size();
+    if ((rc = upload(T.gnode[d], gn.data(), gn.size())) || (rc = upload(T.cmap[d], cm.data(), cm.size()))) return rc;
   }
-  for (int g = 0; g < NN; g++)
-    if (seen[g] != 3) return 1;
+  return 0;
+}
+
+// Phase 2: factorisations.  Every domain's compacted G (for the dE, dH systems and the maps),
+// then the system of the potentials in the reduced form when the domain graph allows it.
+int phase_factor(bem3_ctx c, SolveState& T, const SolveDev& S, Handles& hd)
+{
+  const int MN = c->MN, NN = c->NN;
   int rc;
-  DevBuf dnodes;
-  if ((rc = upload(dnodes, nodes.data(), nodes.size()))) return rc;
-  DevBuf dg[BEM3_MAXDOM], dc[BEM3_MAXDOM];
-  for (int d = 0; d <= MN; d++)
-    if ((rc = upload(dg[d], gnode[d].data(), gnode[d].size())) || (rc = upload(dc[d], cmap[d].data(), cmap[d].size())))
-      return rc;
-  DtnArgs A;
-  A.node = dnodes.as<DtnNode>(); A.geo = S.geo; A.md = S.md; A.sd = S.sd; A.kn = S.kn; A.NN = NN;
-
-  cusolverDnHandle_t hs = nullptr;
-  cublasHandle_t hb = nullptr;
-  if (cusolverDnCreate(&hs) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
-  if (cublasCreate(&hb) != CUBLAS_STATUS_SUCCESS) { cusolverDnDestroy(hs); return BEM3_ERR_CUDA; }
-  struct Handles {
-    cusolverDnHandle_t s; cublasHandle_t b;
-    ~Handles() { cublasDestroy(b); cusolverDnDestroy(s); }
-  } handles{hs, hb};
-
-  // ---- eliminated domains: K_d = G_d^-1 H_d, g^d = G_d^-1 b^d
-  DevBuf Kd[BEM3_MAXDOM], gd[BEM3_MAXDOM];
-  KPtrs KP, GP;
+  bool reduced = (c->solver != 1) && colour_domains(c, T.elim);
+  std::vector<DtnNode> nodes;
+  if (reduced) {
+    nodes.assign((size_t)NN, DtnNode{});
+    std::vector<int> seen((size_t)NN, 0);
+    for (int d = 0; d <= MN; d++) {
+      int j = 0;
+      for (int t = 0; t < (int)c->sid[d].size(); t++) {
+        const int a = abs(c->sid[d][t]);
+        for (int tn = 0; tn < c->nv[a]; tn++, j++) {
+          const int g = c->eni_h[4 * a + tn];
+          if (g < 0 || g >= NN) return BEM3_ERR_ARG;
+          DtnNode& q = nodes[g];
+          q.elem = a; q.l = tn;
+          if (T.elim[d]) { q.de = d; q.le = j; seen[g] |= 1; }
+          else { q.dn = d; q.ln = j; seen[g] |= 2; }
+        }
+      }
+    }
+    for (int g = 0; g < NN; g++)
+      if (seen[g] != 3) reduced = false;
+  }
+  if (!reduced && c->solver == 2) return BEM3_ERR_ARG;  // reduced form asked for but not applicable
+  // compacted G of every domain; the reduced form needs the eliminated domains' K_d first (from
+  // the factorised G_d) and the kept domains' G_e unfactorised for their rows
+  for (int d = 0; d <= MN; d++) {
+    const int n = T.n[d], N = 4 * (int)c->sid[d].size();
+    if (T.Gc[d].alloc((size_t)n * n * 16)) return BEM3_ERR_CUDA;
+    T.bytes += (size_t)n * n * 16;
+    k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.G[d], N, T.cmap[d].as<int>(), n, T.Gc[d].as<double>());
+  }
+  KPtrs KP;
   memset(&KP, 0, sizeof KP);
-  memset(&GP, 0, sizeof GP);
+  if (reduced) {
+    if ((rc = upload(T.nodes, nodes.data(), nodes.size()))) return rc;
+    for (int d = 0; d <= MN; d++) {
+      if (!T.elim[d]) continue;
+      const int n = T.n[d], N = 4 * (int)c->sid[d].size();
+      if ((rc = lu_factor_cm(hd.s, T.Gc[d].as<double>(), n, T.Gpiv[d]))) return rc;
+      if (T.K[d].alloc((size_t)n * n * 16)) return BEM3_ERR_CUDA;
+      T.bytes += (size_t)n * n * 16;
+      k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.H[d], N, T.cmap[d].as<int>(), n, T.K[d].as<double>());
+      if ((rc = lu_solve_cm(hd.s, T.Gc[d].as<double>(), n, T.Gpiv[d], T.K[d].as<double>(), n))) return rc;
+      KP.K[d] = T.K[d].as<double>(); KP.n[d] = n;
+    }
+    const DtnArgs A = dtn_view(c, T, S);
+    const long long na = 4LL * NN;
+    if (T.A.alloc((size_t)na * na * 16)) return BEM3_ERR_CUDA;
+    T.bytes += (size_t)na * na * 16;
+    long long row0 = 0;
+    for (int e = 0; e <= MN; e++) {
+      if (T.elim[e]) continue;
+      const int n = T.n[e], N = 4 * (int)c->sid[e].size();
+      DevBuf Hc, Kh, P, Q;
+      if (Hc.alloc((size_t)n * n * 16) || Kh.alloc((size_t)n * NN * 16) || P.alloc((size_t)n * NN * 16) ||
+          Q.alloc((size_t)n * NN * 16))
+        return BEM3_ERR_CUDA;
+      k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.H[e], N, T.cmap[e].as<int>(), n, Hc.as<double>());
+      k_dtn_khat<<<nblk((long long)n * NN, 256), 256>>>(A, KP, T.gnode[e].as<int>(), n, e, 0, Kh.as<double>());
+      if ((rc = zgemm_nn(hd.b, n, NN, n, T.Gc[e].as<double>(), n, Kh.as<double>(), n, 0.0, P.as<double>(), n))) return rc;
+      k_dtn_khat<<<nblk((long long)n * NN, 256), 256>>>(A, KP, T.gnode[e].as<int>(), n, e, 1, Kh.as<double>());
+      if ((rc = zgemm_nn(hd.b, n, NN, n, T.Gc[e].as<double>(), n, Kh.as<double>(), n, 0.0, Q.as<double>(), n))) return rc;
+      k_dtn_rows<<<nblk(4LL * n * na, 256), 256>>>(A, e, T.gnode[e].as<int>(), n, Hc.as<double>(), T.Gc[e].as<double>(),
+                                                   P.as<double>(), Q.as<double>(), T.A.as<double>(), na, row0);
+      if ((rc = lu_factor_cm(hd.s, T.Gc[e].as<double>(), n, T.Gpiv[e]))) return rc;
+      row0 += 4LL * n;
+    }
+    if (row0 != na) return BEM3_ERR_ARG;
+    if ((rc = lu_factor_cm(hd.s, T.A.as<double>(), (int)na, T.Apiv))) return rc;
+    T.method = 2;
+    return 0;
+  }
+  for (int d = 0; d <= MN; d++)
+    if ((rc = lu_factor_cm(hd.s, T.Gc[d].as<double>(), T.n[d], T.Gpiv[d]))) return rc;
+  // the reference's system, rows in create_tmatrix_csr order, stored row-major (solved transposed)
+  const long long na = 8LL * NN;
+  std::vector<int4> rowmap;
+  rowmap.reserve((size_t)na);
+  for (int d = 0; d <= MN; d++)
+    for (int cid = 0; cid < 4; cid++)
+      for (int t = 0; t < (int)c->sid[d].size(); t++) {
+        const int nv = c->nv[abs(c->sid[d][t])];
+        for (int tn = 0; tn < nv; tn++) rowmap.push_back(make_int4(d, cid, t, tn));
+      }
+  if ((long long)rowmap.size() != na) return BEM3_ERR_ARG;
+  DevBuf drow, scratchB;
+  if ((rc = upload(drow, rowmap.data(), rowmap.size()))) return rc;
+  if (T.A.alloc((size_t)na * na * 16) || scratchB.alloc((size_t)na * 16)) return BEM3_ERR_CUDA;
+  T.bytes += (size_t)na * na * 16;
+  cudaMemset(T.A.p, 0, (size_t)na * na * 16);
+  k_build_rows<<<(unsigned)na, 256>>>(S, drow.as<int4>(), T.A.as<double>(), scratchB.as<double>(), na);
+  if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
+  // row-major A is A^T column-major: factorising that and solving with the transpose gives A x = b
+  if ((rc = lu_factor_cm(hd.s, T.A.as<double>(), (int)na, T.Apiv))) return rc;
+  T.method = 1;
+  return 0;
+}
+
+int lu_solve_cm_t(cusolverDnHandle_t h, const double* A, int n, DevBuf& ipiv, double* B, int nrhs)
+{
+  DevBuf info;
+  if (info.alloc(sizeof(int))) return BEM3_ERR_CUDA;
+  if (cusolverDnZgetrs(h, CUBLAS_OP_T, n, nrhs, (const cuDoubleComplex*)A, n, ipiv.as<int>(), (cuDoubleComplex*)B, n,
+                       info.as<int>()) != CUSOLVER_STATUS_SUCCESS)
+    return BEM3_ERR_SOLVE;
+  int hinfo = 0;
+  if (cudaMemcpy(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return BEM3_ERR_CUDA;
+  return hinfo == 0 ? 0 : BEM3_ERR_SOLVE;
+}
+
+// Phase 3: the incident field's right-hand sides, the potentials, then E, H and dE, dH.
+int phase_rhs(bem3_ctx c, SolveState& T, const SolveDev& S, Handles& hd)
+{
+  const int MN = c->MN, NN = c->NN;
+  int rc;
+  const long long nx = 8LL * NN;
+  DevBuf X, B[BEM3_MAXDOM];
+  if (X.alloc((size_t)nx * 16)) return BEM3_ERR_CUDA;
   for (int d = 0; d <= MN; d++) {
-    if (!elim[d]) continue;
-    const int n = (int)gnode[d].size();
-    const int N = 4 * S.ne[d];
-    DevBuf Gc, ipiv;
-    if (Gc.alloc((size_t)n * n * 16) || Kd[d].alloc((size_t)n * n * 16) || gd[d].alloc((size_t)n * 4 * 16))
-      return BEM3_ERR_CUDA;
-    k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.G[d], N, dc[d].as<int>(), n, Gc.as<double>());
-    k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.H[d], N, dc[d].as<int>(), n, Kd[d].as<double>());
-    k_dtn_rhs<<<dim3(n, 4), 256>>>(S, d, dc[d].as<int>(), n, gd[d].as<double>());
-    if ((rc = lu_factor_cm(hs, Gc.as<double>(), n, ipiv))) return rc;
-    if ((rc = lu_solve_cm(hs, Gc.as<double>(), n, ipiv, Kd[d].as<double>(), n))) return rc;
-    if ((rc = lu_solve_cm(hs, Gc.as<double>(), n, ipiv, gd[d].as<double>(), 4))) return rc;
-    KP.K[d] = Kd[d].as<double>(); KP.n[d] = n;
-    GP.K[d] = gd[d].as<double>(); GP.n[d] = n;
+    if (B[d].alloc((size_t)T.n[d] * 4 * 16)) return BEM3_ERR_CUDA;
+    k_dtn_rhs<<<dim3(T.n[d], 4), 256>>>(S, d, T.cmap[d].as<int>(), T.n[d], B[d].as<double>());
   }
-  // ---- kept domains: their rows of the reduced system
-  const long long na = 4LL * NN;
-  DevBuf Ared, rhs;
-  if (Ared.alloc((size_t)na * na * 16) || rhs.alloc((size_t)na * 16)) return BEM3_ERR_CUDA;
-  long long row0 = 0;
-  for (int e = 0; e <= MN; e++) {
-    if (elim[e]) continue;
-    const int n = (int)gnode[e].size();
-    const int N = 4 * S.ne[e];
-    DevBuf Gc, Hc, Kh, P, Q, b, Gh;
-    if (Gc.alloc((size_t)n * n * 16) || Hc.alloc((size_t)n * n * 16) || Kh.alloc((size_t)n * NN * 16) ||
-        P.alloc((size_t)n * NN * 16) || Q.alloc((size_t)n * NN * 16) || b.alloc((size_t)n * 4 * 16) ||
-        Gh.alloc((size_t)n * 4 * 16))
-      return BEM3_ERR_CUDA;
-    k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.G[e], N, dc[e].as<int>(), n, Gc.as<double>());
-    k_compact_cm<<<nblk((long long)n * n, 256), 256>>>(S.H[e], N, dc[e].as<int>(), n, Hc.as<double>());
-    k_dtn_khat<<<nblk((long long)n * NN, 256), 256>>>(A, KP, dg[e].as<int>(), n, e, 0, Kh.as<double>());
-    if ((rc = zgemm_nn(hb, n, NN, n, Gc.as<double>(), n, Kh.as<double>(), n, 0.0, P.as<double>(), n))) return rc;
-    k_dtn_khat<<<nblk((long long)n * NN, 256), 256>>>(A, KP, dg[e].as<int>(), n, e, 1, Kh.as<double>());
-    if ((rc = zgemm_nn(hb, n, NN, n, Gc.as<double>(), n, Kh.as<double>(), n, 0.0, Q.as<double>(), n))) return rc;
-    k_dtn_rows<<<nblk(4LL * n * na, 256), 256>>>(A, e, dg[e].as<int>(), n, Hc.as<double>(), Gc.as<double>(),
-                                                 P.as<double>(), Q.as<double>(), Ared.as<double>(), na, row0);
-    k_dtn_rhs<<<dim3(n, 4), 256>>>(S, e, dc[e].as<int>(), n, b.as<double>());
-    k_dtn_ghat<<<nblk(4LL * n, 256), 256>>>(A, GP, dg[e].as<int>(), n, e, Gh.as<double>());
-    if ((rc = zgemm_nn(hb, n, 4, n, Gc.as<double>(), n, Gh.as<double>(), n, 1.0, b.as<double>(), n))) return rc;
-    // b is n x 4 column-major: exactly the reduced rows' order c n + j
-    if (cudaMemcpy(rhs.as<double>() + 2 * row0, b.p, (size_t)n * 4 * 16, cudaMemcpyDeviceToDevice) != cudaSuccess)
-      return BEM3_ERR_CUDA;
-    row0 += 4LL * n;
+  if (T.method == 2) {
+    const DtnArgs A = dtn_view(c, T, S);
+    KPtrs GP;
+    memset(&GP, 0, sizeof GP);
+    for (int d = 0; d <= MN; d++) {  // g^d = G_d^-1 b^d (in place)
+      if (!T.elim[d]) continue;
+      if ((rc = lu_solve_cm(hd.s, T.Gc[d].as<double>(), T.n[d], T.Gpiv[d], B[d].as<double>(), 4))) return rc;
+      GP.K[d] = B[d].as<double>(); GP.n[d] = T.n[d];
+    }
+    const long long na = 4LL * NN;
+    DevBuf rhs;
+    if (rhs.alloc((size_t)na * 16)) return BEM3_ERR_CUDA;
+    long long row0 = 0;
+    for (int e = 0; e <= MN; e++) {
+      if (T.elim[e]) continue;
+      const int n = T.n[e], N = 4 * (int)c->sid[e].size();
+      DevBuf Gh;
+      if (Gh.alloc((size_t)n * 4 * 16)) return BEM3_ERR_CUDA;
+      k_dtn_ghat<<<nblk(4LL * n, 256), 256>>>(A, GP, T.gnode[e].as<int>(), n, e, Gh.as<double>());
+      k_compact_matvec4<<<n, 256>>>(S.G[e], N, T.cmap[e].as<int>(), n, Gh.as<double>(), B[e].as<double>());
+      if (cudaMemcpy(rhs.as<double>() + 2 * row0, B[e].p, (size_t)n * 4 * 16, cudaMemcpyDeviceToDevice) != cudaSuccess)
+        return BEM3_ERR_CUDA;
+      row0 += 4LL * n;
+    }
+    if ((rc = lu_solve_cm(hd.s, T.A.as<double>(), (int)na, T.Apiv, rhs.as<double>(), 1))) return rc;
+    for (int d = 0; d <= MN; d++) {
+      if (!T.elim[d]) continue;
+      const int n = T.n[d];
+      DevBuf Ud, KU;
+      if (Ud.alloc((size_t)n * 4 * 16) || KU.alloc((size_t)n * 4 * 16)) return BEM3_ERR_CUDA;
+      k_dtn_gather_u<<<nblk(4LL * n, 256), 256>>>(T.gnode[d].as<int>(), n, NN, rhs.as<double>(), Ud.as<double>());
+      if ((rc = zgemm_nn(hd.b, n, 4, n, T.K[d].as<double>(), n, Ud.as<double>(), n, 0.0, KU.as<double>(), n))) return rc;
+      k_dtn_du<<<nblk(n, 128), 128>>>(A, d, T.gnode[d].as<int>(), n, KU.as<double>(), B[d].as<double>(),
+                                      rhs.as<double>(), X.as<double>());
+    }
+  } else if (T.method == 1) {
+    // right-hand side of the full system in its row order: domain by domain, component-major
+    long long off = 0;
+    for (int d = 0; d <= MN; d++) {
+      if (cudaMemcpy(X.as<double>() + 2 * off, B[d].p, (size_t)T.n[d] * 4 * 16, cudaMemcpyDeviceToDevice) !=
+          cudaSuccess)
+        return BEM3_ERR_CUDA;
+      off += 4LL * T.n[d];
+    }
+    if ((rc = lu_solve_cm_t(hd.s, T.A.as<double>(), (int)nx, T.Apiv, X.as<double>(), 1))) return rc;
+  } else {
+    return BEM3_ERR_ARG;
   }
-  if (row0 != na) return BEM3_ERR_ARG;
-  {
-    DevBuf ipiv;
-    if ((rc = lu_factor_cm(hs, Ared.as<double>(), (int)na, ipiv))) return rc;
-    if ((rc = lu_solve_cm(hs, Ared.as<double>(), (int)na, ipiv, rhs.as<double>(), 1))) return rc;
-  }
-  // ---- dU from the eliminated domains' relations
+  for (int d = 0; d <= MN; d++) k_store_bv<<<(4 * S.ne[d] + 127) / 128, 128>>>(S, d, X.as<double>());
+  // boundary fields E, H (interior domains, and the open-region side of their nodes)
+  for (int d = 1; d <= MN; d++) k_eh_interior<<<(4 * S.ne[d] * 32 + 255) / 256, 256>>>(S, d);
+  // normal derivatives: G_d [dE dH] = H_d [E H] with the factorised compacted G_d
   for (int d = 0; d <= MN; d++) {
-    if (!elim[d]) continue;
-    const int n = (int)gnode[d].size();
-    DevBuf Ud, KU;
-    if (Ud.alloc((size_t)n * 4 * 16) || KU.alloc((size_t)n * 4 * 16)) return BEM3_ERR_CUDA;
-    k_dtn_gather_u<<<nblk(4LL * n, 256), 256>>>(dg[d].as<int>(), n, NN, rhs.as<double>(), Ud.as<double>());
-    if ((rc = zgemm_nn(hb, n, 4, n, Kd[d].as<double>(), n, Ud.as<double>(), n, 0.0, KU.as<double>(), n))) return rc;
-    k_dtn_du<<<nblk(n, 128), 128>>>(A, d, dg[d].as<int>(), n, KU.as<double>(), gd[d].as<double>(), rhs.as<double>(), X);
+    const int nn = T.n[d];
+    DevBuf dBd;
+    if (dBd.alloc((size_t)nn * 6 * 16)) return BEM3_ERR_CUDA;
+    k_deh_system<<<nn, 256>>>(S, d, T.cmap[d].as<int>(), nn, nullptr, dBd.as<double>());
+    if ((rc = lu_solve_cm(hd.s, T.Gc[d].as<double>(), nn, T.Gpiv[d], dBd.as<double>(), 6))) return rc;
+    k_deh_store<<<(nn + 127) / 128, 128>>>(S, d, T.cmap[d].as<int>(), nn, dBd.as<double>());
   }
   if (cudaDeviceSynchronize() != cudaSuccess) return BEM3_ERR_CUDA;
   return 0;
@@ -384,82 +541,65 @@ extern "C" int bem3_ctx_solve(bem3_ctx c)
 {
   if (!c) return BEM3_ERR_ARG;
   DeviceGuard g(c->dev);
-  const int MN = c->MN, NN = c->NN;
-  int rc = 0;
-  SolveDev S = solve_view(c);
-  // ---- assembly of every domain (kept for the system and the dE, dH step)
-  DevBuf dGm[BEM3_MAXDOM], dHm[BEM3_MAXDOM], ddG[BEM3_MAXDOM], ddH[BEM3_MAXDOM], ddF[BEM3_MAXDOM];
-  for (int d = 0; d <= MN; d++) {
-    const int ne = S.ne[d];
-    const size_t N = (size_t)4 * ne;
-    if (dGm[d].alloc(N * N * 16) || dHm[d].alloc(N * N * 16) || ddG[d].alloc(2 * N * N * 16) ||
-        ddH[d].alloc(2 * N * N * 16) || ddF[d].alloc(N * 3 * 8))
-      return BEM3_ERR_CUDA;
-    const int periodic = (d == 0 && c->ps == 1) ? 1 : 0;
-    rc = bem3_assemble_domain_dev(c->geo.as<double>(), c->Ne, c->dsid[d].as<int>(), ne, d, periodic, &c->qd,
-                                  c->kn[2 * d], c->kn[2 * d + 1], dGm[d].as<double>(), dHm[d].as<double>(),
-                                  ddG[d].as<double>(), ddH[d].as<double>(), ddF[d].as<double>(), nullptr);
-    if (rc) return rc;
-    S.G[d] = dGm[d].as<double>(); S.H[d] = dHm[d].as<double>();
-    S.dG[d] = ddG[d].as<double>(); S.dH[d] = ddH[d].as<double>(); S.dF[d] = ddF[d].as<double>();
+  delete c->st;
+  c->st = new SolveState();
+  SolveState& T = *c->st;
+  int rc = phase_assemble(c, T);
+  if (rc) { delete c->st; c->st = nullptr; return rc; }
+  SolveDev S = solve_view_with(c, T);
+  Handles hd;
+  if ((rc = hd.init()) || (rc = phase_factor(c, T, S, hd)) || (rc = phase_rhs(c, T, S, hd))) {
+    delete c->st;
+    c->st = nullptr;
+    return rc;
   }
-  // ---- global system of the potentials: reduced (4 NN) where the domain graph allows it, else
-  //      the reference's full system (8 NN, create_tmatrix_csr row order)
-  {
-    const long long na = (long long)8 * NN;
-    DevBuf X;
-    if (X.alloc((size_t)na * 16)) return BEM3_ERR_CUDA;
-    rc = (c->solver == 1) ? 1 : dtn_solve(c, S, X.as<double>());
-    if (rc == 1 && c->solver == 2) return BEM3_ERR_ARG;  // reduced system asked for but not applicable
-    if (rc == 1) {
-      std::vector<int4> rowmap;
-      rowmap.reserve((size_t)na);
-      for (int d = 0; d <= MN; d++)
-        for (int cid = 0; cid < 4; cid++)
-          for (int t = 0; t < S.ne[d]; t++) {
-            const int nv = c->nv[abs(c->sid[d][t])];
-            for (int tn = 0; tn < nv; tn++) rowmap.push_back(make_int4(d, cid, t, tn));
-          }
-      if ((long long)rowmap.size() != na) return BEM3_ERR_ARG;
-      DevBuf drow, dA;
-      if ((rc = upload(drow, rowmap.data(), rowmap.size()))) return rc;
-      if (dA.alloc((size_t)na * na * 16)) return BEM3_ERR_CUDA;
-      cudaMemset(dA.p, 0, (size_t)na * na * 16);
-      k_build_rows<<<(unsigned)na, 256>>>(S, drow.as<int4>(), dA.as<double>(), X.as<double>(), na);
-      if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
-      cusolverDnHandle_t h = nullptr;
-      if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
-      rc = lu_solve_rowmajor(h, dA.as<double>(), (int)na, X.as<double>(), 1);
-      cusolverDnDestroy(h);
-    }
-    if (rc) return rc;
-    for (int d = 0; d <= MN; d++) k_store_bv<<<(4 * S.ne[d] + 127) / 128, 128>>>(S, d, X.as<double>());
-  }
-  // ---- boundary fields E, H (interior domains, and the open-region side of their nodes)
-  for (int d = 1; d <= MN; d++) k_eh_interior<<<(4 * S.ne[d] * 32 + 255) / 256, 256>>>(S, d);
-  // ---- normal derivatives dE, dH per domain
-  cusolverDnHandle_t h = nullptr;
-  if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
-  for (int d = 0; d <= MN && rc == 0; d++) {
-    std::vector<int> cmap;
-    for (int t = 0; t < S.ne[d]; t++) {
-      const int nv = c->nv[abs(c->sid[d][t])];
-      for (int tn = 0; tn < nv; tn++) cmap.push_back(4 * t + tn);
-    }
-    const int nn = (int)cmap.size();
-    DevBuf dc, dAd, dBd;
-    if ((rc = upload(dc, cmap.data(), cmap.size()))) break;
-    if (dAd.alloc((size_t)nn * nn * 16) || dBd.alloc((size_t)nn * 6 * 16)) { rc = BEM3_ERR_CUDA; break; }
-    k_deh_system<<<nn, 256>>>(S, d, dc.as<int>(), nn, dAd.as<double>(), dBd.as<double>());
-    rc = lu_solve_rowmajor(h, dAd.as<double>(), nn, dBd.as<double>(), 6);
-    if (rc) break;
-    k_deh_store<<<(nn + 127) / 128, 128>>>(S, d, dc.as<int>(), nn, dBd.as<double>());
-  }
-  cusolverDnDestroy(h);
-  if (rc) return rc;
-  if (cudaDeviceSynchronize() != cudaSuccess) return BEM3_ERR_CUDA;
   return 0;
 }
+
+extern "C" int bem3_ctx_set_incident(bem3_ctx c, int nwaves, const bem3_wave* waves, const double* Ui,
+                                     const double* dUi, const double* dEiz, const double* dEie)
+{
+  if (!c || nwaves < 0 || (nwaves > 0 && !waves) || !Ui || !dUi || !dEiz || !dEie) return BEM3_ERR_ARG;
+  DeviceGuard g(c->dev);
+  const size_t Ne1 = (size_t)c->Ne + 1;
+  if (cudaMemcpy(c->Ui.p, Ui, Ne1 * 32 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->dUi.p, dUi, Ne1 * 32 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->dEiz.p, dEiz, Ne1 * 24 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->dEie.p, dEie, Ne1 * 24 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return BEM3_ERR_CUDA;
+  if (nwaves > 0) {
+    DevBuf w;
+    int rc = upload(w, waves, (size_t)nwaves);
+    if (rc) return rc;
+    std::swap(c->waves.p, w.p);
+  }
+  c->nwaves = nwaves;
+  return 0;
+}
+
+extern "C" int bem3_ctx_resolve(bem3_ctx c)
+{
+  if (!c) return BEM3_ERR_ARG;
+  if (!c->st || !c->st->method) return bem3_ctx_solve(c);
+  DeviceGuard g(c->dev);
+  SolveState& T = *c->st;
+  SolveDev S = solve_view_with(c, T);
+  Handles hd;
+  int rc = hd.init();
+  if (!rc) rc = phase_rhs(c, T, S, hd);
+  return rc;
+}
+
+extern "C" int bem3_ctx_release(bem3_ctx c)
+{
+  if (!c) return BEM3_ERR_ARG;
+  DeviceGuard g(c->dev);
+  delete c->st;
+  c->st = nullptr;
+  return 0;
+}
+
+extern "C" size_t bem3_ctx_device_bytes(bem3_ctx c) { return (c && c->st) ? c->st->bytes : 0; }
 
 namespace {
 

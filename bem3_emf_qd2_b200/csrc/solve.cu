@@ -258,12 +258,12 @@ __global__ void k_deh_system(SolveDev S, int d, const int* __restrict__ cmap, in
   const size_t N = (size_t)4 * ne;
   const double* G = S.G[d] + 2 * ((size_t)src * N);
   const double* H = S.H[d] + 2 * ((size_t)src * N);
-  double* Ar = A + 2 * (size_t)c * nn;
+  double* Ar = A ? A + 2 * (size_t)c * nn : nullptr;  // A == nullptr: right-hand sides only
   cplx acc[6];
   for (int j = 0; j < 6; j++) acc[j] = mk(0, 0);
   for (int r = threadIdx.x; r < nn; r += blockDim.x) {
     const int col = cmap[r];
-    stc(Ar, r, ldc(G, col));
+    if (Ar) stc(Ar, r, ldc(G, col));
     const int s = col >> 2, sn = col & 3;
     cplx h = ldc(H, col);
     const size_t b3 = (size_t)(4 * (s + 1) + sn) * 3;

@@ -228,3 +228,28 @@ __global__ void k_dtn_du(DtnArgs A, int d, const int* __restrict__ gnode, int n_
   cplx nU = U[0] * nrm[0] + U[1] * nrm[1] + U[2] * nrm[2];
   stc(X, 7 * NN + m, cdiv(q3 - sigm * nU, beps));
 }
+
+// Y (n x 4, column-major) += G_d,compact X, G_d read in place from the domain's row-major
+// 4ne x 4ne matrix through cmap; one CTA per row.
+__global__ void k_compact_matvec4(const double* __restrict__ G, int N, const int* __restrict__ cmap, int n,
+                                  const double* __restrict__ X, double* __restrict__ Y)
+{
+  const int i = blockIdx.x;
+  const double* row = G + 2 * ((size_t)cmap[i] * N);
+  cplx acc[4];
+  for (int c = 0; c < 4; c++) acc[c] = mk(0, 0);
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const cplx g = ldc(row, cmap[j]);
+    for (int c = 0; c < 4; c++) acc[c] += g * ldc(X, (size_t)c * n + j);
+  }
+  __shared__ double red[8][256];
+  for (int c = 0; c < 4; c++) { red[2 * c][threadIdx.x] = acc[c].re; red[2 * c + 1][threadIdx.x] = acc[c].im; }
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 8; k++) red[k][threadIdx.x] += red[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int c = 0; c < 4; c++) stc(Y, (size_t)c * n + i, ldc(Y, (size_t)c * n + i) + mk(red[2 * c][0], red[2 * c + 1][0]));
+}

@@ -311,15 +311,32 @@ class Problem:
                     wv = w[:, 0] + w[:, 1] * z + w[:, 2] * e
                 self.ren[i, j] = r
                 self.wen[i, j] = wv
+        self._incident()
+
+    def _incident(self):
         nrm = self.wen / np.linalg.norm(self.wen, axis=-1, keepdims=True).clip(1e-300)
         self.Ui = np.zeros((self.Ne + 1, 4, 4), np.complex128)
         self.dUi = np.zeros((self.Ne + 1, 4, 4), np.complex128)
-        for w in waves:
+        for w in self.waves:
             e, h, de, dh = w.eh_dehdv(self.ren, nrm)
             self.Ui[..., :3] += e
             self.dUi[..., :3] += de
         self.Ui[0] = 0
         self.dUi[0] = 0
+
+    def with_waves(self, waves) -> "Problem":
+        """The same geometry and media under other incident plane waves with the same wavelength,
+        background index and direction (so the same lattice phase and matrices)."""
+        import copy
+        for w in waves:
+            w.setup()
+            if (w.lambda0 != self.lambda0 or w.ni != self.n0 or w.theta != self.waves[0].theta
+                    or w.phi != self.waves[0].phi):
+                raise ValueError("a new incident field must keep the wavelength, index and direction")
+        q = copy.copy(self)
+        q.waves = list(waves)
+        q._incident()
+        return q
 
     def node_tangents(self):
         """Unit tangents t_zeta, t_eta at every collocation node (tz_te_bd_node,

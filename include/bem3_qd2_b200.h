@@ -196,6 +196,19 @@ int bem3_ctx_solve(bem3_ctx c);
  * which always solves the 8 NN system with PARDISO. */
 int bem3_ctx_set_solver(bem3_ctx c, int method);
 
+/* A solve leaves the matrices and factorisations on the device (bem3_ctx_device_bytes says how
+ * much).  A new incident field with the same wavelength and direction (another polarisation, a
+ * different amplitude or phase; the matrices depend on the wavelength and on k||) then needs
+ * only its right-hand sides: bem3_ctx_set_incident replaces the incident data of bem3_problem
+ * (same layouts), bem3_ctx_resolve recomputes the boundary values.  bem3_ctx_release frees the
+ * matrices and factorisations and keeps the boundary values.  No counterpart in the reference,
+ * which assembles and factorises for every run. */
+int bem3_ctx_set_incident(bem3_ctx c, int nwaves, const bem3_wave *waves, const double *Ui, const double *dUi,
+                          const double *dEiz, const double *dEie);
+int bem3_ctx_resolve(bem3_ctx c);
+int bem3_ctx_release(bem3_ctx c);
+size_t bem3_ctx_device_bytes(bem3_ctx c);
+
 /* Boundary values to host arrays (layout of bem3_bv), or from host arrays (for example the
  * values a reference result file holds, read by dat_read d3qd2_setup.c:300). */
 int bem3_ctx_get_bv(bem3_ctx c, bem3_bv *out /* [MN+1] */);
