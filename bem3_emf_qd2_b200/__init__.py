@@ -24,8 +24,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libbem3qd2.so")
 REPO = os.path.dirname(HERE)
 
+# --default-stream per-thread: work the library issues without an explicit stream goes to the calling
+# host thread's own default stream, so contexts driven from different threads overlap on the GPU.
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-diag-suppress", "20091", "-Xcompiler", "-fPIC", "-shared"]
+              "--default-stream", "per-thread", "-diag-suppress", "20091", "-Xcompiler", "-fPIC", "-shared"]
 
 ERRORS = {
     -1: "invalid argument", -2: "CUDA failure", -3: "scratch too small", -4: "degenerate lattice",

@@ -23,8 +23,9 @@ struct DevRes {
   QPProp* prop = nullptr;               // propagating orders of the lattice being assembled
 };
 
-std::mutex g_mu;
-DevRes g_res[MAX_DEV];
+// One set per host thread and device: concurrent assemblies from different threads (each on its
+// own stream) never share scratch.  A thread's scratch is kept until the process exits.
+thread_local DevRes t_res[MAX_DEV];
 thread_local bem3_stats t_last_stats;
 thread_local int t_profiling = 0;
 
@@ -40,7 +41,7 @@ int ensure_scratch(size_t bytes, DevRes** out)
 {
   int d = cur_dev();
   if (d < 0 || d >= MAX_DEV) return BEM3_ERR_ARG;
-  DevRes& r = g_res[d];
+  DevRes& r = t_res[d];
   if (!r.status) {
     if (cudaMalloc(&r.status, sizeof(int)) != cudaSuccess) return BEM3_ERR_CUDA;
   }
@@ -184,7 +185,6 @@ extern "C" int bem3_assemble_domain_dev(const double* geo_dev, int Ne, const int
   cudaStream_t st = (cudaStream_t)stream;
   int rows = default_rows_per_chunk(Ne_d);
   size_t need = bem3_scratch_bytes(Ne_d, rows);
-  std::lock_guard<std::mutex> lk(g_mu);
   DevRes* R = nullptr;
   int e = ensure_scratch(need, &R);
   if (e) return e;

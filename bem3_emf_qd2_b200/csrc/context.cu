@@ -151,7 +151,7 @@ extern "C" int bem3_ctx_create(const bem3_problem* P, bem3_ctx* out)
     cudaMemset(c->dE[d].p, 0, bv3_bytes(ne)); cudaMemset(c->dH[d].p, 0, bv3_bytes(ne));
   }
   if (c->status.alloc(sizeof(int))) return fail(BEM3_ERR_CUDA);
-  if (cudaDeviceSynchronize() != cudaSuccess) return fail(BEM3_ERR_CUDA);
+  if (cudaStreamSynchronize(cudaStreamPerThread) != cudaSuccess) return fail(BEM3_ERR_CUDA);
   *out = c;
   return 0;
 }
@@ -276,8 +276,12 @@ struct Handles {
   cublasHandle_t b = nullptr;
   int init()
   {
+    // the libraries' own default is the legacy stream, which would serialise with every thread
     if (cusolverDnCreate(&s) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
     if (cublasCreate(&b) != CUBLAS_STATUS_SUCCESS) return BEM3_ERR_CUDA;
+    if (cusolverDnSetStream(s, cudaStreamPerThread) != CUSOLVER_STATUS_SUCCESS ||
+        cublasSetStream(b, cudaStreamPerThread) != CUBLAS_STATUS_SUCCESS)
+      return BEM3_ERR_CUDA;
     return 0;
   }
   ~Handles()
@@ -524,7 +528,7 @@ int phase_rhs(bem3_ctx c, SolveState& T, const SolveDev& S, Handles& hd)
     if ((rc = lu_solve_cm(hd.s, T.Gc[d].as<double>(), nn, T.Gpiv[d], dBd.as<double>(), 6))) return rc;
     k_deh_store<<<(nn + 127) / 128, 128>>>(S, d, T.cmap[d].as<int>(), nn, dBd.as<double>());
   }
-  if (cudaDeviceSynchronize() != cudaSuccess) return BEM3_ERR_CUDA;
+  if (cudaStreamSynchronize(cudaStreamPerThread) != cudaSuccess) return BEM3_ERR_CUDA;
   return 0;
 }
 

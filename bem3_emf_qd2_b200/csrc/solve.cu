@@ -303,10 +303,21 @@ __global__ void k_deh_store(SolveDev S, int d, const int* __restrict__ cmap, int
 
 namespace {
 
+// Device buffer from the stream-ordered allocator on the calling thread's default stream: freeing
+// it does not synchronise the device (cudaFree would wait for every stream), so contexts used from
+// different host threads do not stall each other.  Every user of a buffer has finished, in that
+// stream's order, before the buffer goes out of scope.
 struct DevBuf {
   void* p = nullptr;
-  ~DevBuf() { if (p) cudaFree(p); }
-  int alloc(size_t bytes) { return cudaMalloc(&p, bytes) == cudaSuccess ? 0 : BEM3_ERR_CUDA; }
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { if (p) cudaFreeAsync(p, cudaStreamPerThread); }
+  int alloc(size_t bytes)
+  {
+    if (p) { cudaFreeAsync(p, cudaStreamPerThread); p = nullptr; }
+    return cudaMallocAsync(&p, bytes, cudaStreamPerThread) == cudaSuccess ? 0 : BEM3_ERR_CUDA;
+  }
   template <class T> T* as() { return (T*)p; }
 };
 

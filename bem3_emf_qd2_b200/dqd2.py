@@ -247,35 +247,9 @@ class Problem:
         self.Ne = ed.shape[0] - 1
         self.nv = np.where(ed[:, 3] == 0, 3, 4).astype(np.int32)
         self.nv[0] = 4
+        self.media = list(media)
         # initialize_dqd2 (d3qd2_src/d3qd2_setup.c:105-139)
-        for w in waves:
-            w.setup()
-        self.n0 = waves[0].ni
-        self.lambda0 = waves[0].lambda0
-        for w in waves[1:]:
-            if w.ni != self.n0 or w.lambda0 != self.lambda0:
-                raise ValueError("all plane waves must share ni and lambda0")
-        if ps == 1:
-            kx0 = waves[0].sin_t * waves[0].cos_p
-            ky0 = waves[0].sin_t * waves[0].sin_p
-            for w in waves:
-                kxh, kyh, kzh = w.sin_t * w.cos_p, w.sin_t * w.sin_p, w.cos_t
-                if kzh == 0.0:
-                    raise ValueError("kz must not be equal to 0")
-                if abs(kzh) == 1.0:
-                    raise ValueError("kz must not be equal to the wave number (normal incidence)")
-                if abs(kx0 - kxh) > MEPS * abs(kxh) or abs(ky0 - kyh) > MEPS * abs(kyh):
-                    raise ValueError("all kx and ky must be the same")
-        w0 = waves[0]
-        k = w0.ki
-        vk = [k * w0.sin_t * w0.cos_p, k * w0.sin_t * w0.sin_p, k * w0.cos_t]
-        if vk[0] == 0.0:
-            vk[0] = k * MEPS
-        if vk[1] == 0.0:
-            vk[1] = k * MEPS
-        self.qpd = dict(k=k, vk=vk, vd1=vd1, vd2=vd2)
-        self.n = [complex(self.n0)] + list(media)
-        self.kn = [2.0 * math.pi / self.lambda0 * nd for nd in self.n]
+        self._waves_setup(waves)
         self.cr, self.cw = element_constants(rn, ed)
         # sub-domains (init_sub_domain, d3qd2_setup.c:1290-1307)
         self.sid = []
@@ -312,6 +286,49 @@ class Problem:
                 self.ren[i, j] = r
                 self.wen[i, j] = wv
         self._incident()
+
+    def _waves_setup(self, waves):
+        """Wave-dependent part of initialize_dqd2: check_mipw (d3qd2_setup.c:1078-1108), the QPGF
+        data, the wave numbers of the media (:120-129)."""
+        for w in waves:
+            w.setup()
+        self.waves = waves
+        self.n0 = waves[0].ni
+        self.lambda0 = waves[0].lambda0
+        for w in waves[1:]:
+            if w.ni != self.n0 or w.lambda0 != self.lambda0:
+                raise ValueError("all plane waves must share ni and lambda0")
+        if self.ps == 1:
+            kx0 = waves[0].sin_t * waves[0].cos_p
+            ky0 = waves[0].sin_t * waves[0].sin_p
+            for w in waves:
+                kxh, kyh, kzh = w.sin_t * w.cos_p, w.sin_t * w.sin_p, w.cos_t
+                if kzh == 0.0:
+                    raise ValueError("kz must not be equal to 0")
+                if abs(kzh) == 1.0:
+                    raise ValueError("kz must not be equal to the wave number (normal incidence)")
+                if abs(kx0 - kxh) > MEPS * abs(kxh) or abs(ky0 - kyh) > MEPS * abs(kyh):
+                    raise ValueError("all kx and ky must be the same")
+        w0 = waves[0]
+        k = w0.ki
+        vk = [k * w0.sin_t * w0.cos_p, k * w0.sin_t * w0.sin_p, k * w0.cos_t]
+        if vk[0] == 0.0:
+            vk[0] = k * MEPS
+        if vk[1] == 0.0:
+            vk[1] = k * MEPS
+        self.qpd = dict(k=k, vk=vk, vd1=self.vd1, vd2=self.vd2)
+        self.n = [complex(self.n0)] + list(self.media)
+        self.kn = [2.0 * math.pi / self.lambda0 * nd for nd in self.n]
+
+    def with_incidence(self, waves) -> "Problem":
+        """The same geometry and media under any other incident plane waves (wavelength,
+        background index, angles, polarisation): the problem read_dqd2 + initialize_dqd2 would
+        build from the same mesh and a different ipw file, without repeating the geometry."""
+        import copy
+        q = copy.copy(self)
+        q._waves_setup(list(waves))
+        q._incident()
+        return q
 
     def _incident(self):
         nrm = self.wen / np.linalg.norm(self.wen, axis=-1, keepdims=True).clip(1e-300)

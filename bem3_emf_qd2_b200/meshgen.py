@@ -206,6 +206,11 @@ def make_config(name: str, outdir: str, **over):
     their paths (ipw, periodicity, medium, mesh)."""
     cfg = dict(CONFIGS[name])
     cfg.update(over)
+    return write_config(name, cfg, outdir)
+
+
+def write_config(name: str, cfg: dict, outdir: str):
+    """make_config for a configuration dictionary of the same form as CONFIGS' entries."""
     nodes = _Nodes()
     surfs = []
     for s in cfg["surfaces"]:

@@ -82,7 +82,8 @@ int bem3_assemble_domain(const bem3_mesh *mesh, const int *sid, int Ne_d, int di
 
 /* Device-resident variant.  geo_dev: packed geometry from bem3_pack_geometry (uploaded by the
  * caller); sid_dev: [Ne_d] ints; outputs in device memory.  The library allocates its scratch
- * (bem3_assemble_scratch_bytes) with cudaMalloc on first use and keeps it for later calls. */
+ * with cudaMalloc on a calling thread's first use and keeps it, per host thread and device, for
+ * that thread's later calls; calls from different threads may run concurrently. */
 int bem3_assemble_domain_dev(const double *geo_dev, int Ne, const int *sid_dev, int Ne_d, int did, int periodic,
                              const bem3_qpd2 *qd, double kre, double kim, double *G_dev, double *H_dev,
                              double *dG_dev, double *dH_dev, double *dF_dev, void *stream);
@@ -177,8 +178,9 @@ int bem3_solve_bieq_arrays(const bem3_problem *P, bem3_bv *out /* [MN+1] */);
 /* ---------------------------------------------------------------------------------------------
  * Device-resident problem.  A context holds one problem's geometry, media, incident waves and
  * boundary values on the current CUDA device, so that a solve and any number of field
- * evaluations share one upload.  Contexts are independent of each other; one context must not
- * be used from two threads at once. */
+ * evaluations share one upload.  Contexts are independent of each other: each call's work goes
+ * to the calling host thread's default stream, so contexts driven from different threads run
+ * concurrently on the GPU.  One context must not be used from two threads at once. */
 typedef struct bem3_ctx_s *bem3_ctx;
 
 /* Copies the problem to the device.  The caller's arrays may be freed afterwards. */
