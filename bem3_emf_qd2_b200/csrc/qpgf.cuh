@@ -97,6 +97,23 @@ BEM_HD_NOINLINE double qp_erfc(double x) { return erfc(x); }
 #else
 BEM_HD double qp_erfc(double x) { return erfc(x); }
 #endif
+// e^{x^2} erfc(x) for x >= 0.  The host form (the host builds of these headers are test code)
+// uses the product below x = 25 and the asymptotic series above, where it converges to ~1e-18.
+BEM_HD double qp_erfcx(double x)
+{
+#if defined(__CUDA_ARCH__)
+  return erfcx(x);
+#else
+  if (x < 25.0) return exp(x * x) * erfc(x);
+  const double t = 1.0 / (2.0 * x * x);
+  double s = 1.0, term = 1.0;
+  for (int k = 1; k <= 10; k++) {
+    term *= -(2.0 * k - 1.0) * t;
+    s += term;
+  }
+  return s / (x * 1.7724538509055160273);
+#endif
+}
 #if defined(QP_EXP_NOINLINE)
 BEM_HD_NOINLINE double qp_exp(double x) { return exp(x); }
 #else
@@ -155,21 +172,43 @@ BEM_HD void qp_ew2_prop(const double* r, double veps, double an0, double an1, do
   dF[2] = 2.0 * (ce * mk(ef * w.re - ff.re, -ff.im));
 }
 // ibn = 1/bn: the evaluation forms below differ only in how they obtain bn and 1/bn.
+// FAST: with a = bn veps and b = z / (2 veps) (so that bn z = 2 a b),
+//   e^{bn z} erfc(a + b)  = e^{-a^2 - b^2} erfcx(a + b)
+//   e^{-bn z} erfc(a - b) = e^{-a^2 - b^2} erfcx(a - b)                 (a >= b)
+//                         = 2 e^{-bn z} - e^{-a^2 - b^2} erfcx(b - a)    (a <  b)
+// (erfcx(x) = e^{x^2} erfc(x), erfc(-x) = 2 - erfc(x)): one shared exponential and two scaled
+// complementary error functions of non-negative arguments instead of two erfc (each an exponential
+// inside), an exponential and a division.
+template <bool FAST = false>
 BEM_HD void qp_ew2_evan(const double* r, double veps, double an0, double an1, double bn, double ibn, cplx ce, cplx& F,
                         cplx* dF)
 {
   BEM_STAT_T(2);
   double azve = r[2] / (2.0 * veps);
-  double ebz = qp_exp(bn * r[2]);
-  // both erfc values from one call site (one copy of its code in the sums)
-  double e1 = 0.0, e2 = 0.0;
+  double f1, f2;
+  if (FAST) {
+    const double a = bn * veps;
+    const double E = qp_exp(-(a * a + azve * azve));
+    double x1 = 0.0, x2 = 0.0;
 #pragma unroll 1
-  for (int j = 0; j < 2; j++) {
-    const double v = qp_erfc(j == 0 ? bn * veps + azve : bn * veps - azve);
-    if (j == 0) e1 = v; else e2 = v;
+    for (int j = 0; j < 2; j++) {
+      const double v = qp_erfcx(j == 0 ? a + azve : fabs(a - azve));
+      if (j == 0) x1 = v; else x2 = v;
+    }
+    f1 = E * x1;
+    f2 = (a >= azve) ? E * x2 : 2.0 * qp_exp(-bn * r[2]) - E * x2;
+  } else {
+    double ebz = qp_exp(bn * r[2]);
+    // both erfc values from one call site (one copy of its code in the sums)
+    double e1 = 0.0, e2 = 0.0;
+#pragma unroll 1
+    for (int j = 0; j < 2; j++) {
+      const double v = qp_erfc(j == 0 ? bn * veps + azve : bn * veps - azve);
+      if (j == 0) e1 = v; else e2 = v;
+    }
+    f1 = ebz * e1;
+    f2 = 1.0 / ebz * e2;
   }
-  double f1 = ebz * e1;
-  double f2 = 1.0 / ebz * e2;
   // Fn = ce / (i bn) (f1 + f2) = -i ce (f1+f2)/bn
   F = mul_mi(ce * ((f1 + f2) * ibn));
   dF[0] = F * an0;
@@ -188,7 +227,7 @@ BEM_HD int qp_ew2_term(const QPLattice& L, const double* r, double veps, int n1,
     return 0;
   } else if (bn2 < 0.0) {
     const double bn = sqrt(-bn2);
-    qp_ew2_evan(r, veps, an0, an1, bn, 1.0 / bn, ce, F, dF);
+    qp_ew2_evan<FAST>(r, veps, an0, an1, bn, 1.0 / bn, ce, F, dF);
     return 1;
   }
   return -3;
@@ -370,7 +409,7 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
         const double ibn = rsqrt_(-bn2);
         const double bn = -bn2 * ibn;
         if (FD) qp_fd_evan(r, an0, an1, bn, ibn, ph, F, dF);
-        else qp_ew2_evan(r, veps, an0, an1, bn, ibn, ph, F, dF);
+        else qp_ew2_evan<OPT>(r, veps, an0, an1, bn, ibn, ph, F, dF);
         e = 1;
       } else {
         e = FD ? -2 : -3;
