@@ -245,6 +245,40 @@ def _bv_arrays(problem: Problem):
     return out, bvs
 
 
+def plane_power(field, vd1, vd2, upward: bool, z_top: float, z_bottom: float, n: int = 16):
+    """Time-averaged power through one unit cell of the lattice, from the fields on the planes
+    z = z_top (above the objects) and z = z_bottom (below), each sampled on an n x n grid of the
+    cell and integrated with the midpoint rule (spectrally accurate: Re(E x H*) is periodic and
+    smooth away from the objects).  field(r, total) -> (E, H, did) evaluates EH_t (total) or EH_s.
+    Returns P_inc (incident field through the entry plane), P_ref (scattered field leaving
+    through the entry plane), P_tra (total field leaving through the other plane) and
+    balance = (P_ref + P_tra) / P_inc, which is 1 for lossless objects.  The Poynting vector is
+    Re(E x H*) / 2 in the units of E and H."""
+    d1 = np.array([vd1[0], vd1[1], 0.0])
+    d2 = np.array([vd2[0], vd2[1], 0.0])
+    u = (np.arange(n) + 0.5) / n
+    grid = (u[:, None, None] * d1 + u[None, :, None] * d2).reshape(-1, 3)
+    area = abs(d1[0] * d2[1] - d1[1] * d2[0])
+
+    def fields(z, total):
+        E, H, did = field(grid + np.array([0.0, 0.0, z]), total)
+        if np.any(np.asarray(did) != 0):
+            raise ValueError("the planes must lie in the open region")
+        return E, H
+
+    def flux(E, H):
+        return (0.5 * (E[:, 0] * np.conj(H[:, 1]) - E[:, 1] * np.conj(H[:, 0])).real).mean() * area
+
+    up = 1.0 if upward else -1.0  # the incident wave travels along +z or -z
+    zin, zout = (z_bottom, z_top) if upward else (z_top, z_bottom)
+    Et, Ht = fields(zin, True)
+    Es, Hs = fields(zin, False)
+    P_inc = up * flux(Et - Es, Ht - Hs)
+    P_ref = -up * flux(Es, Hs)
+    P_tra = up * flux(*fields(zout, True))
+    return dict(P_inc=P_inc, P_ref=P_ref, P_tra=P_tra, balance=(P_ref + P_tra) / P_inc)
+
+
 class Context:
     """A problem resident on the current CUDA device (bem3_ctx): solve, boundary values, fields."""
 
@@ -316,6 +350,13 @@ class Context:
         N = np.zeros(3)
         check(lib().bem3_ctx_force(self.h, _ptr(rc), type_, _ptr(F), _ptr(N)), "bem3_ctx_force")
         return F, N
+
+    def power(self, z_top: float, z_bottom: float, n: int = 16, type_: int = 0):
+        """Reflected and transmitted power through one unit cell (plane_power) from this context's
+        fields."""
+        p = self.p
+        return plane_power(lambda r, total: self.field(r, type_, total), p.vd1, p.vd2, p.waves[0].cos_t > 0,
+                           z_top, z_bottom, n)
 
     def field(self, r, type_: int = 0, total: bool = True):
         """E, H [n,3] complex and the domain of each point (EH_t if total else EH_s)."""

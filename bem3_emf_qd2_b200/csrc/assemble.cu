@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleA
 }
 
 // Near-singular periodic pairs: one CTA (256 threads) per listed pair, 64x64 rule.
-__global__ void __launch_bounds__(256, 1) k_gh_periodic(AssembleArgs A, const __grid_constant__ QPLattice L, long long p0, double3* Fp,
+__global__ void __launch_bounds__(256, 2) k_gh_periodic(AssembleArgs A, const __grid_constant__ QPLattice L, long long p0, double3* Fp,
                                                      const unsigned* gh_list, const unsigned* gh_count, int* status)
 {
   __shared__ double red[8][19];
@@ -387,7 +387,7 @@ __global__ void k_rowsum(AssembleArgs A, int row0, int nrows, const double3* Fp,
 // q0_lit_dcoef_bd_vt2_cc_DV q0_lit_dcoef_v2_cc.c:331-342).  One CTA per (t, tn); the point loop
 // and the combination are self_per_points / self_per_combine (self.cuh).
 #define SELF_THREADS 256
-__global__ void __launch_bounds__(SELF_THREADS, 1) k_self_periodic(AssembleArgs A, const __grid_constant__ QPLattice L, double3* Fself, int* status)
+__global__ void __launch_bounds__(SELF_THREADS, 2) k_self_periodic(AssembleArgs A, const __grid_constant__ QPLattice L, double3* Fself, int* status)
 {
   __shared__ double red[SELF_THREADS / 32][24];
   __shared__ int serr[SELF_THREADS / 32];

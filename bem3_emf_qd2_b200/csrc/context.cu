@@ -656,9 +656,10 @@ extern "C" int bem3_ctx_domain_id(bem3_ctx c, int n, const double* r, int* did)
 
 extern "C" int bem3_ctx_field(bem3_ctx c, int n, const double* r, int type, int total, double* E, double* H, int* did)
 {
-  if (!c || n < 0 || (n > 0 && (!r || !E || !H)) || (type != 0 && type != 1)) return BEM3_ERR_ARG;
+  if (!c || n < 0 || (n > 0 && (!r || !E || !H)) || type < 0 || type > 3) return BEM3_ERR_ARG;
   if (n == 0) return 0;
   DeviceGuard g(c->dev);
+  if (type >= 2 && ensure_tables() != 0) return BEM3_ERR_CUDA;  // Gauss-Legendre tables
   FieldArgs A = field_view(c);
   DevBuf dr, ddid, dcell, dE, dH;
   int rc = run_domain_id(c, A, n, r, dr, ddid, dcell);

@@ -123,11 +123,12 @@ __global__ void __launch_bounds__(FIELD_THREADS) k_field(FieldArgs A, const __gr
   const int ne = A.ne[d];
   const int* sid = A.sid[d];
   const double *bE = A.E[d], *bdE = A.dE[d], *bH = A.H[d], *bdH = A.dH[d];
+  const FieldGL gl = {c_xl, c_wl, c_xh, c_wh};
   for (int s = threadIdx.x; s < ne; s += FIELD_THREADS) {
     cplx CC[8];
     double f;
-    const int st = per ? field_coef<true>(A.geo, sid[s], rt, k, type, L, CC, f)
-                       : field_coef<false>(A.geo, sid[s], rt, k, type, L, CC, f);
+    const int st = per ? field_coef<true>(A.geo, sid[s], rt, k, type, L, CC, f, &gl)
+                       : field_coef<false>(A.geo, sid[s], rt, k, type, L, CC, f, &gl);
     if (st < 0) record_status(status, st);
     const size_t b = (size_t)(4 * (s + 1)) * 3;
     for (int nn = 0; nn < 4; nn++) {

@@ -8,6 +8,8 @@
 //   type 0: the element's own collocation nodes (4-point rule on quads, the 4-point
 //           triangle rule with the centroid on triangles)
 //   type 1: 3x3 Gauss rule on quads, 7-point rule on triangles
+//   types 2 and 3: 12 x 12 and 64 x 64 Gauss-Legendre rules (field_coef_gl), for points near
+//           the boundary
 // (q0_bil_coef_4p/_9p q0_bil_coef.c:10-95, q0_lit_coef_4p/_7p q0_lit_coef.c:10-117 for the
 // periodic Green's function; bil_coef_4p/_9p bil_coef.c:25-97, lit_coef_4p/_7p lit_coef.c:26-123
 // for the free-space one.)  Each quadrature point's Green's function is evaluated once and
@@ -97,13 +99,65 @@ BEM_HD int field_kernel(const QPLattice& L, cplx k, const double* vR, const doub
 // shape functions), CC[4..7] (normal derivative), F.  Triangles leave CC[3], CC[7] zero.
 // Returns 0, a QPGF failure code, or -1 for an unsupported type or a negative id in the
 // periodic region (the reference exits there, q0_bil_coef.c:16-19).
+// Gauss-Legendre tables for the rules of types 2 and 3: x12, w12, x64, w64.
+struct FieldGL {
+  const double *x12, *w12, *x64, *w64;
+};
+
+// Types 2 (12 x 12 Gauss-Legendre, 3 x 12 x 12 on triangles) and 3 (64 x 64): the same quadrature
+// sums as the regular element rules of the assembly (q0_bil_coef_GL/_GH q0_bil_coef.c:97-190,
+// q0_lit_coef_GL/_GH q0_lit_coef.c:118-250, bil_coef_GL/_GH bil_coef.c:99-190, lit_coef_GL/_GH
+// lit_coef.c:125-260), so they run through accp_point / acci_point and keep their CC part.
+template <bool PER>
+BEM_HD int field_coef_gl(const double* geo, int sd, const double* rt, cplx k, int type, const FieldGL& gl,
+                         const QPLattice& L, cplx* CC, double& F)
+{
+  const int s = sd < 0 ? -sd : sd;
+  Elem el;
+  load_elem(geo, s, el);
+  const int n = (type == 2) ? 12 : 64;
+  const double* x = (type == 2) ? gl.x12 : gl.x64;
+  const double* w = (type == 2) ? gl.w12 : gl.w64;
+  const int npts = (el.nn == 4) ? n * n : 3 * n * n;
+  const double v0[3] = {0.0, 0.0, 0.0};  // tangents of the derivative parts, not needed here
+  cplx C9[9], dCz[9], dCe[9];
+  int err = 0;
+  if (PER) {
+    AccP a;
+    accp_zero(a);
+    for (int q = 0; q < npts; q++) {
+      double z, e, wt;
+      rule_point(el.nn, n, x, w, q, z, e, wt);
+      const int st = accp_point(el, L, rt, v0, v0, z, e, wt, a);
+      if (st < 0) err = st;
+    }
+    accp_finish(el, a, C9, dCz, dCe);
+  } else {
+    AccI a;
+    acci_zero(a);
+    for (int q = 0; q < npts; q++) {
+      double z, e, wt;
+      rule_point(el.nn, n, x, w, q, z, e, wt);
+      acci_point(el, k, rt, v0, v0, z, e, wt, a);
+    }
+    acci_finish(el, a, sd < 0, C9, dCz, dCe);
+  }
+  for (int i = 0; i < 8; i++) CC[i] = C9[i];
+  F = C9[8].re;
+  return err;
+}
+
 template <bool PER>
 BEM_HD int field_coef(const double* geo, int sd, const double* rt, cplx k, int type, const QPLattice& L, cplx* CC,
-                      double& F)
+                      double& F, const FieldGL* gl = nullptr)
 {
   for (int i = 0; i < 8; i++) CC[i] = mk(0.0, 0.0);
   F = 0.0;
   if (PER && sd < 0) return -1;
+  if (type == 2 || type == 3) {
+    if (!gl) return -1;
+    return field_coef_gl<PER>(geo, sd, rt, k, type, *gl, L, CC, F);
+  }
   if (type != 0 && type != 1) return -1;
   const int s = sd < 0 ? -sd : sd;
   const double* g = geo + (size_t)s * GEO_STRIDE;

@@ -221,7 +221,9 @@ int bem3_ctx_domain_id(bem3_ctx c, int n, const double *r, int *did);
 
 /* Electromagnetic field at n points (EH_s / EH_t, d3qd2_src/d3qd2_field.c:203-285).
  * r: [n][3]; E, H: [n][3] complex; did: [n] domain of each point (may be NULL).
- * type 0: nodal 4-point rules, type 1: 9-point (quads) / 7-point (triangles) rules.
+ * type 0: nodal 4-point rules, type 1: 9-point (quads) / 7-point (triangles) rules, types 2 and
+ * 3: 12 x 12 and 64 x 64 Gauss-Legendre rules (three sub-quads on triangles), for points near the
+ * boundary.  (The reference's type 4, double-exponential integration, is not provided.)
  * total != 0 adds the incident field in the open region (EH_t), else scattered/internal (EH_s).
  * Points outside every domain get did = -1 and zero fields. */
 int bem3_ctx_field(bem3_ctx c, int n, const double *r, int type, int total, double *E, double *H, int *did);

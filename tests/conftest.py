@@ -41,7 +41,7 @@ def devmath_host():
     lib.hm_pair_regular.restype = i
     lib.hm_self_interior.argtypes = [vp, i, i, d, d, vp, vp, vp, vp, vp]
     lib.hm_self_periodic.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp]
-    lib.hm_field_coef.argtypes = [vp, i, vp, i, d, d, i, vp, vp]
+    lib.hm_field_coef.argtypes = [vp, i, vp, i, d, d, i, vp, vp, vp]
     lib.hm_solid_angle.argtypes = [vp, vp, i, i, vp, vp]
     lib.hm_solid_angle.restype = d
     lib.hm_self_periodic.restype = i

@@ -14,9 +14,13 @@ from its sources by oracle/Makefile and called through oracle/reforacle.py:
                 the reference ships (verification/veri.dat, analysis_sample*/ex*.dat), read by its
                 own dat_read, plus the reference's EH_t (d3qd2_field.c) at probe points and its
                 force_FN (d3qd2_force.c) for those results, types 0 and 1.
+  near_fields.npz  the reference's EH_t, types 0-3, at points just off the boundary of those
+                results.
+  power.npz     incident, reflected and transmitted power through one unit cell for those
+                results, from the reference's EH_t / EH_s on two planes.
 
 Usage: python tests/golden/make_golden.py [reference_dir] [section ...]
-       sections: gauleg faddeeva qpgf rows bv (default: all)
+       sections: gauleg faddeeva qpgf rows bv near power (default: all)
 """
 import os
 import sys
@@ -32,7 +36,8 @@ from reforacle import RefOracle  # noqa: E402
 from bem3_emf_qd2_b200.dqd2 import load_inputs  # noqa: E402
 
 REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-SECTIONS = {a for a in sys.argv[2:] if "=" not in a} or {"gauleg", "faddeeva", "qpgf", "rows", "bv"}
+SECTIONS = {a for a in sys.argv[2:] if "=" not in a} or {"gauleg", "faddeeva", "qpgf", "rows", "bv", "near",
+                                                         "power"}
 ONLY = {x for a in sys.argv[2:] if a.startswith("only=") for x in a[5:].split(",")}
 
 
@@ -111,8 +116,67 @@ def bv_fixtures(o):
         print(name, "bv done", flush=True)
 
 
+def near_fields(o):
+    """EH_t of the reference, types 0-3, at points just off the boundary (both sides) of a few
+    elements of each shipped result file."""
+    out = {}
+    for name, (sub, dat, msh, rot, pts) in BV_CASES.items():
+        o.load_dat(os.path.join(REF, sub, dat))
+        g = o.geometry()
+        ne = g["cr"].shape[0] - 1
+        pick = [1, ne // 3, (2 * ne) // 3]
+        r = []
+        for e in pick:
+            c = g["cr"][e, :, 0]
+            w = g["cw"][e, :, 0]
+            h = np.sqrt(np.linalg.norm(w))
+            n = w / np.linalg.norm(w)
+            for f in (0.1, -0.1, 0.3):
+                r.append(c + f * h * n)
+        r = np.array(r)
+        out[name + "/r"] = r
+        for ty in (0, 1, 2, 3):
+            E, H, did = o.EH(r, ty, total=True)
+            out[f"{name}/E{ty}"] = E
+            out[f"{name}/H{ty}"] = H
+            out[f"{name}/did"] = did
+        print(name, "near fields done", flush=True)
+    np.savez_compressed(os.path.join(HERE, "near_fields.npz"), **out)
+
+
+POWER = {"veri": (1.4, -1.4, 16), "ex2": (1.2, -1.2, 16)}  # z_top, z_bottom, grid
+
+
+def power_balance(o):
+    """Reflected, transmitted and incident power through one cell from the reference's EH_t/EH_s
+    sampled on two planes (the same quadrature as bem3_emf_qd2_b200.plane_power)."""
+    from bem3_emf_qd2_b200 import plane_power
+    from bem3_emf_qd2_b200.dqd2 import problem_from_arrays
+    out = {}
+    for name, (sub, dat, msh, rot, pts) in BV_CASES.items():
+        o.load_dat(os.path.join(REF, sub, dat))
+        g = np.load(os.path.join(HERE, f"bv_{name}.npz"))
+        p = problem_from_arrays({k[3:]: g[k] for k in g.files if k.startswith("in/")})
+        zt, zb, n = POWER[name]
+
+        def field(r, total):
+            E, H, did = o.EH(r, 0, total=total)
+            return E, H, did
+
+        res = plane_power(field, p.vd1, p.vd2, p.waves[0].cos_t > 0, zt, zb, n)
+        out[name + "/spec"] = np.array([zt, zb, n])
+        for k, v in res.items():
+            out[f"{name}/{k}"] = np.array(v)
+        print(name, res, flush=True)
+    np.savez_compressed(os.path.join(HERE, "power.npz"), **out)
+
+
 def main():
     o = RefOracle()
+    if "power" in SECTIONS:
+        power_balance(o)
+    if "near" in SECTIONS:
+        near_fields(o)
     if "gauleg" in SECTIONS:
         gauleg_tables(o)
     if "bv" in SECTIONS:

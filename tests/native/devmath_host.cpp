@@ -145,15 +145,20 @@ extern "C" {
 
 // Field coefficients of source element sd at point rt with the device rules (field.cuh);
 // out = CC[0..7] re/im pairs then F.  Returns the status of field_coef.
+// gl: x12, w12, x64, w64 (152 doubles) for types 2 and 3.
 int hm_field_coef(const double* geo, int sd, const double* rt, int periodic, double kre, double kim, int type,
-                  const double* p, double* out)
+                  const double* p, const double* gl, double* out)
 {
   QPLattice L;
   qp_lattice_init(L, p[0], p[1], p[2], p[4], p[5], p[6], p[7]);
+  static thread_local QPProp prop[QP_PROP_CAP];
+  L.nprop = qp_prop_list(L, prop, QP_PROP_CAP);
+  L.prop = prop;
+  const FieldGL tabs = {gl, gl + 12, gl + 24, gl + 88};
   cplx CC[8];
   double F;
-  int st = periodic ? field_coef<true>(geo, sd, rt, mk(kre, kim), type, L, CC, F)
-                    : field_coef<false>(geo, sd, rt, mk(kre, kim), type, L, CC, F);
+  int st = periodic ? field_coef<true>(geo, sd, rt, mk(kre, kim), type, L, CC, F, &tabs)
+                    : field_coef<false>(geo, sd, rt, mk(kre, kim), type, L, CC, F, &tabs);
   for (int i = 0; i < 8; i++) { out[2 * i] = CC[i].re; out[2 * i + 1] = CC[i].im; }
   out[16] = F;
   return st;

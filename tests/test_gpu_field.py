@@ -78,3 +78,21 @@ def test_scattered_plus_incident_is_total(cuda_lib):
         e_inc += w.eh_dehdv(r[out], np.zeros_like(r[out]))[0]
     assert np.abs(Et[out] - Es[out] - e_inc).max() <= 1e-13 * np.abs(e_inc).max()
     ctx.close()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_near_boundary_fields_all_rules(cuda_lib, name):
+    """Points at 0.1 and 0.3 element sizes off the boundary, rules of types 0-3, against the
+    reference's EH_t with the same boundary values: |E - E_ref| <= 1e-9 * max|E_ref|."""
+    g, p = _case(name)
+    near = golden("near_fields.npz")
+    r = near[f"{name}/r"]
+    ctx = cuda_lib.Context(p)
+    ctx.set_boundary_values(_ref_bv(g, p))
+    for ty in (0, 1, 2, 3):
+        E, H, did = ctx.field(r, ty, total=True)
+        assert np.array_equal(did, near[f"{name}/did"])
+        for got, key in ((E, f"{name}/E{ty}"), (H, f"{name}/H{ty}")):
+            ref = near[key]
+            assert np.abs(got - ref).max() <= 1e-9 * np.abs(ref).max(), (ty, key)
+    ctx.close()
