@@ -271,25 +271,46 @@ bool colour_domains(bem3_ctx c, std::vector<int>& elim)
   return true;
 }
 
+// cuSOLVER / cuBLAS handles, created once per host thread and device and kept (creating them
+// costs milliseconds, more than a small problem's whole solve stage).
 struct Handles {
   cusolverDnHandle_t s = nullptr;
   cublasHandle_t b = nullptr;
   int init()
   {
     // the libraries' own default is the legacy stream, which would serialise with every thread
-    if (cusolverDnCreate(&s) != CUSOLVER_STATUS_SUCCESS) return BEM3_ERR_CUDA;
-    if (cublasCreate(&b) != CUBLAS_STATUS_SUCCESS) return BEM3_ERR_CUDA;
+    if (!s && cusolverDnCreate(&s) != CUSOLVER_STATUS_SUCCESS) { s = nullptr; return BEM3_ERR_CUDA; }
+    if (!b && cublasCreate(&b) != CUBLAS_STATUS_SUCCESS) { b = nullptr; return BEM3_ERR_CUDA; }
     if (cusolverDnSetStream(s, cudaStreamPerThread) != CUSOLVER_STATUS_SUCCESS ||
         cublasSetStream(b, cudaStreamPerThread) != CUBLAS_STATUS_SUCCESS)
       return BEM3_ERR_CUDA;
     return 0;
   }
-  ~Handles()
+};
+
+// One set per device, released when the thread ends (the main thread's before the runtime's
+// own teardown at exit).
+struct ThreadHandles {
+  Handles h[64];
+  ~ThreadHandles()
   {
-    if (b) cublasDestroy(b);
-    if (s) cusolverDnDestroy(s);
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) return;
+    for (int d = 0; d < 64; d++) {
+      if (!h[d].s && !h[d].b) continue;
+      if (cudaSetDevice(d) != cudaSuccess) continue;
+      if (h[d].b) cublasDestroy(h[d].b);
+      if (h[d].s) cusolverDnDestroy(h[d].s);
+    }
+    cudaSetDevice(cur);
   }
 };
+
+Handles& thread_handles(int dev)
+{
+  static thread_local ThreadHandles t;
+  return t.h[(dev >= 0 && dev < 64) ? dev : 0];
+}
 
 DtnArgs dtn_view(bem3_ctx c, const SolveState& T, const SolveDev& S)
 {
@@ -551,7 +572,7 @@ extern "C" int bem3_ctx_solve(bem3_ctx c)
   int rc = phase_assemble(c, T);
   if (rc) { delete c->st; c->st = nullptr; return rc; }
   SolveDev S = solve_view_with(c, T);
-  Handles hd;
+  Handles& hd = thread_handles(c->dev);
   if ((rc = hd.init()) || (rc = phase_factor(c, T, S, hd)) || (rc = phase_rhs(c, T, S, hd))) {
     delete c->st;
     c->st = nullptr;
@@ -588,7 +609,7 @@ extern "C" int bem3_ctx_resolve(bem3_ctx c)
   DeviceGuard g(c->dev);
   SolveState& T = *c->st;
   SolveDev S = solve_view_with(c, T);
-  Handles hd;
+  Handles& hd = thread_handles(c->dev);
   int rc = hd.init();
   if (!rc) rc = phase_rhs(c, T, S, hd);
   return rc;

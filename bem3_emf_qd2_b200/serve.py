@@ -352,10 +352,10 @@ def main():
     meshes, probes = mesh_pool(tempfile.mkdtemp(prefix="bem3_pool_"))
     backend = GpuBackend(probes)
     budget = int(args.budget_gb * 1e9)
-    # warm-up: one small solve loads the library's kernels and the solver libraries
-    small = min(meshes, key=lambda k: meshes[k].NN)
-    w = request_stream({small: meshes[small]}, 1, None)
-    run_sequential(meshes, backend, w)
+    # warm-up: one solve per pooled mesh loads the library's kernels and the solver libraries'
+    # kernels for every system size the pool reaches (modules load lazily, on first launch)
+    for name in sorted(meshes):
+        run_sequential(meshes, backend, request_stream({name: meshes[name]}, 1, None))
 
     seq = None
     reqs0 = request_stream(meshes, args.requests, None)
