@@ -79,7 +79,8 @@ class bem3_bv(C.Structure):
 
 class bem3_stats(C.Structure):
     _fields_ = [("gh_pairs", C.c_ulonglong), ("qpgf_terms", C.c_ulonglong), ("launches", C.c_int),
-                ("reg_periodic_launches", C.c_int), ("reg_periodic_ms", C.c_double)]
+                ("reg_periodic_launches", C.c_int), ("reg_periodic_ms", C.c_double),
+                ("class_ms", C.c_double * 4)]
 
 
 _lib = None
@@ -390,7 +391,9 @@ def gauss_legendre(n: int):
 def last_stats() -> dict:
     st = bem3_stats()
     lib().bem3_last_stats(C.byref(st))
-    return {f: getattr(st, f) for f, _ in bem3_stats._fields_}
+    out = {f: getattr(st, f) for f, _ in bem3_stats._fields_}
+    out["class_ms"] = list(out["class_ms"])
+    return out
 
 
 def set_profiling(on: bool) -> None:

@@ -509,11 +509,25 @@ int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, 
 
   int launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  const bool timing = stats && stats->time_kernels && A.periodic;
+  const bool timing = stats && stats->time_kernels;
   if (timing) { cudaEventCreate(&ev0); cudaEventCreate(&ev1); }
+  // profiling only: the duration of the kernels launched since tic() goes to class_ms[cls]
+  auto tic = [&]() { if (timing) cudaEventRecord(ev0, st); };
+  auto toc = [&](int cls) -> float {
+    float ms = 0.f;
+    if (timing) {
+      cudaEventRecord(ev1, st);
+      cudaEventSynchronize(ev1);
+      cudaEventElapsedTime(&ms, ev0, ev1);
+      stats->class_ms[cls] += ms;
+    }
+    return ms;
+  };
   // self pairs
+  tic();
   if (A.periodic) k_self_periodic<<<nrows, SELF_THREADS, 0, st>>>(A, *L, Fself, d_status);
   else bem3_launch_self_interior(A, Fself, d_status, st);
+  toc(0);
   launches++;
 
   for (int r0 = 0; r0 < nrows; r0 += rows_per_chunk) {
@@ -523,23 +537,28 @@ int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, 
     if (A.periodic) {
       long long threads = (np + REGP_PAIRS - 1) / REGP_PAIRS * 32;
       unsigned blocks = (unsigned)((threads + 255) / 256);
-      if (timing) cudaEventRecord(ev0, st);
+      tic();
       k_reg_periodic<<<blocks, 256, REGP_SMEM_BYTES, st>>>(A, *L, p0, np, Fp, gh_list, gh_count, gh_cap, d_status);
+      const float ms = toc(1);
       if (timing) {
-        cudaEventRecord(ev1, st);
-        cudaEventSynchronize(ev1);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ev0, ev1);
         stats->reg_periodic_ms += ms;
         stats->reg_periodic_launches++;
       }
+      tic();
       k_gh_periodic<<<148 * 4, 256, 0, st>>>(A, *L, p0, Fp, gh_list, gh_count, d_status);
+      toc(2);
     } else {
       unsigned blocks = (unsigned)((np + 127) / 128);
+      tic();
       k_reg_interior<<<blocks, 128, 0, st>>>(A, p0, np, Fp, gh_list, gh_count, gh_cap, d_status);
+      toc(1);
+      tic();
       k_gh_interior<<<148 * 4, 256, 0, st>>>(A, p0, Fp, gh_list, gh_count);
+      toc(2);
     }
+    tic();
     k_rowsum<<<(nr * 32 + 255) / 256, 256, 0, st>>>(A, r0, nr, Fp, Fself);
+    toc(3);
     launches += 3;
     if (stats) {
       unsigned c = 0;

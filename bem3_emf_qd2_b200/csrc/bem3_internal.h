@@ -26,9 +26,10 @@ struct AssembleArgs {
 struct AssembleStats {
   unsigned long long gh_pairs;   // near-singular pairs recomputed with the 64x64 rule
   int launches;                  // kernels launched
-  int time_kernels;              // in: 1 = time the regular periodic kernel with CUDA events
+  int time_kernels;              // in: 1 = time every kernel with CUDA events (synchronising)
   double reg_periodic_ms;        // out: summed duration of k_reg_periodic launches
   int reg_periodic_launches;     // out: number of k_reg_periodic launches
+  double class_ms[4];            // out: self, regular, near-singular, row-sum kernels (any domain)
 };
 
 size_t bem3_scratch_bytes(int ne, int rows);

@@ -220,6 +220,7 @@ extern "C" int bem3_assemble_domain_dev(const double* geo_dev, int Ne, const int
   t_last_stats.launches = S.launches;
   t_last_stats.reg_periodic_launches = S.reg_periodic_launches;
   t_last_stats.reg_periodic_ms = S.reg_periodic_ms;
+  for (int i = 0; i < 4; i++) t_last_stats.class_ms[i] = S.class_ms[i];
   return hs;
 }
 

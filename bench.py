@@ -36,10 +36,10 @@ UNIT = "pairs/s"
 # terms the kernel's own counter reports for that launch, captured on the workload's /stride8
 # subsample (same lattice, wavelength and element size).  The live roofline figure is
 # terms/s x this number.
-FP64_OPS_PER_TERM = {"twolayer3072": 273.1}
+FP64_OPS_PER_TERM = {"twolayer3072": 240.0}
 # DRAM bytes (read + write) of one k_reg_periodic launch, from the same capture scaled by the
 # pairs processed (64x for stride 8).
-TRAFFIC_PER_LAUNCH = {"twolayer3072": 1.6167e9 * 64}
+TRAFFIC_PER_LAUNCH = {"twolayer3072": 1.5412e9 * 64}
 
 
 def parse():
@@ -252,6 +252,8 @@ def run_ours(args):
     # kernel launches per step and the roofline of the dominant kernel (profiling pass, not timed above)
     B.set_profiling(True)
     reg_ms, reg_launches, terms, per_step_launches, gh = 0.0, 0, 0, 0, 0
+    counts = class_counts(p)
+    classes = {}
     for d in domains:
         dev.assemble(d, sptr)
         st = B.last_stats()
@@ -260,6 +262,17 @@ def run_ours(args):
         terms += st["qpgf_terms"]
         per_step_launches += st["launches"]
         gh += st["gh_pairs"]
+        kd = "periodic" if (d == 0 and p.ps == 1) else "interior"
+        ms_self, ms_reg, ms_gh, ms_sum = st["class_ms"]
+        n_self = counts[(d, kd, "self")]
+        n_reg = counts[(d, kd, "regular")]
+        for cls, n, cms in ((f"{kd}_self", n_self, ms_self), (f"{kd}_regular", n_reg - st["gh_pairs"], ms_reg),
+                            (f"{kd}_near_singular", st["gh_pairs"], ms_gh), ("row_sums", 0, ms_sum)):
+            c = classes.setdefault(cls, {"pairs": 0, "ms": 0.0})
+            c["pairs"] += int(n)
+            c["ms"] += cms
+    for c in classes.values():
+        c["pairs_per_s"] = c["pairs"] / (c["ms"] * 1e-3) if c["pairs"] and c["ms"] > 0 else None
     B.set_profiling(False)
     peak = B.fp64_peak_tflops()
     roof = None
@@ -323,6 +336,7 @@ def run_ours(args):
                        "parallelism": f"{world} independent instances (one per GPU)"},
             "gpu_launches": per_step_launches * args.steps,
             "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
+            "classes": classes,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -110,14 +110,16 @@ int bem3_pack_geometry(const bem3_mesh *mesh, double *geo);
 unsigned long long bem3_last_gh_pairs(void);
 
 /* Profiling counters of the last assembly on this thread.  Filled only after
- * bem3_set_profiling(1) (which adds a per-warp term counter and CUDA-event timing of the
- * regular periodic kernel); otherwise only gh_pairs and launches are set. */
+ * bem3_set_profiling(1) (which adds a per-warp term counter and CUDA-event timing of every
+ * kernel, synchronising after each); otherwise only gh_pairs and launches are set. */
 typedef struct {
   unsigned long long gh_pairs;     /* pairs recomputed with the 64x64 near-singular rule */
   unsigned long long qpgf_terms;   /* lattice-sum terms summed by the regular periodic kernel */
   int launches;                    /* kernels launched by the call */
   int reg_periodic_launches;       /* launches of the regular periodic kernel */
   double reg_periodic_ms;          /* their summed duration (CUDA events) */
+  double class_ms[4];              /* kernel time by pair class: self (t == s), regular,
+                                      near-singular (64x64 rule), row sums of F */
 } bem3_stats;
 void bem3_set_profiling(int on);
 int bem3_last_stats(bem3_stats *out);
