@@ -83,6 +83,16 @@ class bem3_stats(C.Structure):
                 ("class_ms", C.c_double * 4)]
 
 
+class bem3_batch_domain(C.Structure):
+    _fields_ = [("geo", C.c_void_p), ("Ne", C.c_int), ("sid", C.c_void_p), ("Ne_d", C.c_int), ("did", C.c_int),
+                ("periodic", C.c_int), ("qd", bem3_qpd2), ("kre", C.c_double), ("kim", C.c_double),
+                ("G", C.c_void_p), ("H", C.c_void_p), ("dG", C.c_void_p), ("dH", C.c_void_p), ("dF", C.c_void_p)]
+
+
+class bem3_batch_tuning(C.Structure):
+    _fields_ = [("grab_units", C.c_int), ("regp_blocks_per_sm", C.c_int), ("gh_blocks_per_sm", C.c_int)]
+
+
 _lib = None
 
 
@@ -123,6 +133,14 @@ def lib():
         L.bem3_set_profiling.argtypes = [i]
         L.bem3_last_stats.argtypes = [C.POINTER(bem3_stats)]
         L.bem3_fp64_peak_tflops.restype = d
+        L.bem3_batch_scratch_bytes.argtypes = [C.POINTER(bem3_batch_domain), i]
+        L.bem3_batch_scratch_bytes.restype = C.c_size_t
+        L.bem3_batch_create.argtypes = [C.POINTER(bem3_batch_domain), i, C.POINTER(bem3_batch_tuning),
+                                        C.POINTER(C.c_void_p)]
+        L.bem3_batch_run.argtypes = [vp, vp]
+        L.bem3_batch_wait.argtypes = [vp, vp, vp]
+        L.bem3_batch_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_size_t)]
+        L.bem3_batch_destroy.argtypes = [vp]
         _lib = L
     return _lib
 

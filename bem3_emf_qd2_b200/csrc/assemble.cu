@@ -151,22 +151,17 @@ struct RegWarp {
 #define REGP_PAIRS 2  // pairs per warp: 2 x 144 Gauss points = 9 per lane, no ragged last step
 #define REGP_SMEM_BYTES (sizeof(RegWarp) * 8 * REGP_PAIRS + sizeof(AccP) * 256 * REGP_PAIRS)
 
-// Regular periodic pairs: one warp per REGP_PAIRS consecutive pairs of the chunk; lane l takes the
-// points l, l + 32, ... of the pairs' concatenated point lists.
-__global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleArgs A, const __grid_constant__ QPLattice L,
-                                                                       long long p0, long long np, double3* Fp,
-                                                                       unsigned* gh_list, unsigned* gh_count,
-                                                                       unsigned gh_cap, int* status)
+// One warp's unit of regular periodic work: the pairs first, first + 1, ... (REGP_PAIRS of them,
+// those < np) of the chunk that starts at pair p0 of the domain.  Lane l takes the points l, l + 32,
+// ... of the pairs' concatenated point lists.  sw: the warp's REGP_PAIRS pair slots; sacc: the
+// block's per-thread accumulators (shared memory).
+__device__ __forceinline__ void reg_periodic_unit(const AssembleArgs& A, const QPLattice& L, long long p0, long long np,
+                                                  long long first, double3* Fp, unsigned* gh_list, unsigned* gh_count,
+                                                  unsigned gh_cap, int* status, RegWarp* sw, AccP (*sacc)[256], int lane)
 {
-  extern __shared__ __align__(16) unsigned char regp_smem[];  // REGP_SMEM_BYTES
-  RegWarp(*sw)[REGP_PAIRS] = reinterpret_cast<RegWarp(*)[REGP_PAIRS]>(regp_smem);
-  AccP(*sacc)[256] = reinterpret_cast<AccP(*)[256]>(regp_smem + sizeof(RegWarp) * 8 * REGP_PAIRS);
-  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const long long first = w * REGP_PAIRS;  // pair index within the chunk
-  if (first >= np) return;  // uniform across the warp
   int npts[REGP_PAIRS];
   PairIdx q[REGP_PAIRS];
+  __syncwarp();  // a warp that runs several units reuses its slots: the last unit's reads are done
 #pragma unroll
   for (int j = 0; j < REGP_PAIRS; j++) {
     npts[j] = 0;
@@ -175,7 +170,7 @@ __global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleA
     const int at = abs(A.sid[q[j].t]);
     const int tnn = (int)A.geo[(size_t)at * GEO_STRIDE + GEO_NN];
     if ((q[j].tn == 3 && tnn == 3) || q[j].s == q[j].t) continue;
-    RegWarp& W = sw[wib][j];
+    RegWarp& W = sw[j];
     if (lane == 0) {
       int tn_unused;
       target_info(A.geo, A.sid, q[j].t, q[j].tn, W.rt, W.vtz, W.vte, tn_unused);
@@ -191,7 +186,7 @@ __global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleA
   for (int k = lane; k < ntot; k += 32) {
     const int j = (k < npts[0]) ? 0 : 1;
     const int kk = j ? k - npts[0] : k;
-    const RegWarp& W = sw[wib][j];
+    const RegWarp& W = sw[j];
     double z, e, wt;
     rule_point(W.es.nn, 12, c_xl, c_wl, kk, z, e, wt);
     int e2 = accp_point(W.es, L, W.rt, W.vtz, W.vte, z, e, wt, sacc[j][threadIdx.x]);
@@ -213,7 +208,7 @@ __global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleA
     AccP s;
     accp_unpack(v, s);
     cplx CC[9], dCz[9], dCe[9];
-    accp_finish(sw[wib][j].es, s, CC, dCz, dCe);
+    accp_finish(sw[j].es, s, CC, dCz, dCe);
     const long long pi = first + j;
     if (needs_gh(dCz[8].re, dCe[8].re)) {
       if (lane == 0) {
@@ -227,15 +222,28 @@ __global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleA
   }
 }
 
-// Near-singular periodic pairs: one CTA (256 threads) per listed pair, 64x64 rule.
-__global__ void __launch_bounds__(256, 2) k_gh_periodic(AssembleArgs A, const __grid_constant__ QPLattice L, long long p0, double3* Fp,
-                                                     const unsigned* gh_list, const unsigned* gh_count, int* status)
+// Regular periodic pairs of one chunk: one warp per REGP_PAIRS consecutive pairs.
+__global__ void __launch_bounds__(256, REGP_MIN_BLOCKS) k_reg_periodic(AssembleArgs A, const __grid_constant__ QPLattice L,
+                                                                       long long p0, long long np, double3* Fp,
+                                                                       unsigned* gh_list, unsigned* gh_count,
+                                                                       unsigned gh_cap, int* status)
 {
-  __shared__ double red[8][19];
-  __shared__ int serr[8];
-  unsigned n = *gh_count;
-  for (unsigned it = blockIdx.x; it < n; it += gridDim.x) {
-    long long w = gh_list[it];
+  extern __shared__ __align__(16) unsigned char regp_smem[];  // REGP_SMEM_BYTES
+  RegWarp(*sw)[REGP_PAIRS] = reinterpret_cast<RegWarp(*)[REGP_PAIRS]>(regp_smem);
+  AccP(*sacc)[256] = reinterpret_cast<AccP(*)[256]>(regp_smem + sizeof(RegWarp) * 8 * REGP_PAIRS);
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const long long first = w * REGP_PAIRS;  // pair index within the chunk
+  if (first >= np) return;  // uniform across the warp
+  reg_periodic_unit(A, L, p0, np, first, Fp, gh_list, gh_count, gh_cap, status, sw[wib], sacc, lane);
+}
+
+// Near-singular periodic pair w of the chunk starting at pair p0, 64x64 rule, by the whole CTA
+// (256 threads; red, serr: its shared reduction slots).  Every thread of the CTA calls it.
+__device__ __forceinline__ void gh_periodic_pair(const AssembleArgs& A, const QPLattice& L, long long p0, long long w,
+                                                 double3* Fp, int* status, double (*red)[19], int* serr)
+{
+  {
     PairIdx q = pair_of(p0 + w, A.ne);
     int tnn;
     double rt[3], vtz[3], vte[3];
@@ -273,13 +281,23 @@ __global__ void __launch_bounds__(256, 2) k_gh_periodic(AssembleArgs A, const __
   }
 }
 
-// ==========================================================================================
-// Regular interior pairs: one thread per pair.
-__global__ void __launch_bounds__(128) k_reg_interior(AssembleArgs A, long long p0, long long np, double3* Fp,
-                                                      unsigned* gh_list, unsigned* gh_count, unsigned gh_cap, int* status)
+// Near-singular periodic pairs of one chunk: one CTA per listed pair.  The list holds at most
+// gh_cap entries (the counter keeps counting past it; the regular kernel then reports -900).
+__global__ void __launch_bounds__(256, 2) k_gh_periodic(AssembleArgs A, const __grid_constant__ QPLattice L, long long p0, double3* Fp,
+                                                     const unsigned* gh_list, const unsigned* gh_count, unsigned gh_cap,
+                                                     int* status)
 {
-  long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= np) return;
+  __shared__ double red[8][19];
+  __shared__ int serr[8];
+  const unsigned n = min(*gh_count, gh_cap);
+  for (unsigned it = blockIdx.x; it < n; it += gridDim.x) gh_periodic_pair(A, L, p0, gh_list[it], Fp, status, red, serr);
+}
+
+// ==========================================================================================
+// Regular interior pair w of the chunk starting at pair p0, by one thread.
+__device__ __forceinline__ void reg_interior_pair(const AssembleArgs& A, long long p0, long long w, double3* Fp,
+                                                  unsigned* gh_list, unsigned* gh_count, unsigned gh_cap, int* status)
+{
   long long p = p0 + w;
   PairIdx q = pair_of(p, A.ne);
   int tnn;
@@ -309,17 +327,20 @@ __global__ void __launch_bounds__(128) k_reg_interior(AssembleArgs A, long long 
   store_pair(A, q.row, q.s, CC, dCz, dCe, Fp, w, -1);
 }
 
-// Near-singular interior pairs: one warp per listed pair, 64x64 rule.
-__global__ void __launch_bounds__(256) k_gh_interior(AssembleArgs A, long long p0, double3* Fp, const unsigned* gh_list,
-                                                     const unsigned* gh_count)
+// Regular interior pairs of one chunk: one thread per pair.
+__global__ void __launch_bounds__(128) k_reg_interior(AssembleArgs A, long long p0, long long np, double3* Fp,
+                                                      unsigned* gh_list, unsigned* gh_count, unsigned gh_cap, int* status)
 {
-  unsigned n = *gh_count;
-  int lane = threadIdx.x & 31;
-  unsigned wglob = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  unsigned nw = (gridDim.x * blockDim.x) >> 5;
+  long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= np) return;
+  reg_interior_pair(A, p0, w, Fp, gh_list, gh_count, gh_cap, status);
+}
+
+// Near-singular interior pair w of the chunk starting at pair p0, 64x64 rule, by one warp.
+__device__ __forceinline__ void gh_interior_pair(const AssembleArgs& A, long long p0, long long w, double3* Fp, int lane)
+{
   const cplx k = mk(A.kre, A.kim);
-  for (unsigned it = wglob; it < n; it += nw) {
-    long long w = gh_list[it];
+  {
     PairIdx q = pair_of(p0 + w, A.ne);
     int tnn;
     double rt[3], vtz[3], vte[3];
@@ -345,22 +366,29 @@ __global__ void __launch_bounds__(256) k_gh_interior(AssembleArgs A, long long p
   }
 }
 
+// Near-singular interior pairs of one chunk: one warp per listed pair (at most gh_cap of them).
+__global__ void __launch_bounds__(256) k_gh_interior(AssembleArgs A, long long p0, double3* Fp, const unsigned* gh_list,
+                                                     const unsigned* gh_count, unsigned gh_cap)
+{
+  const unsigned n = min(*gh_count, gh_cap);
+  const int lane = threadIdx.x & 31;
+  const unsigned wglob = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nw = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned it = wglob; it < n; it += nw) gh_interior_pair(A, p0, gh_list[it], Fp, lane);
+}
+
 // ==========================================================================================
 // Row sums (d3qd2_solve_bieq.c:222-236): F, dF/dtz, dF/dte over all s (regular pairs from the
 // chunk scratch, the self pair from Fself), then H[row][4t+tn] += (did==0 ? 1 : 0) + F.
 // One warp per row; lane-strided partial sums and a fixed-shape reduction (deterministic).
-__global__ void k_rowsum(AssembleArgs A, int row0, int nrows, const double3* Fp, const double3* Fself)
+// fr: the row's F terms (ne of them, indexed by s).
+__device__ __forceinline__ void rowsum_row(const AssembleArgs& A, int row, const double3* fr, const double3* Fself, int lane)
 {
-  int wr = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (wr >= nrows) return;
-  int row = row0 + wr;
   int t = row >> 2, tn = row & 3;
   int at = abs(A.sid[t]);
   int tnn = (int)A.geo[(size_t)at * GEO_STRIDE + GEO_NN];
   if (tn == 3 && tnn == 3) return;
   double f0 = 0, f1 = 0, f2 = 0;
-  const double3* fr = Fp + (size_t)wr * A.ne;
   for (int s = lane; s < A.ne; s += 32) {
     if (s == t) continue;
     double3 v = fr[s];
@@ -382,16 +410,23 @@ __global__ void k_rowsum(AssembleArgs A, int row0, int nrows, const double3* Fp,
   }
 }
 
+__global__ void k_rowsum(AssembleArgs A, int row0, int nrows, const double3* Fp, const double3* Fself)
+{
+  int wr = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (wr >= nrows) return;
+  rowsum_row(A, row0 + wr, Fp + (size_t)wr * A.ne, Fself, lane);
+}
+
 // ==========================================================================================
 // Self pairs of the periodic domain (q0_bil_dcoef_bd_vt2_cc_DV q0_bil_dcoef_v2_cc.c:292-301 and
 // q0_lit_dcoef_bd_vt2_cc_DV q0_lit_dcoef_v2_cc.c:331-342).  One CTA per (t, tn); the point loop
 // and the combination are self_per_points / self_per_combine (self.cuh).
 #define SELF_THREADS 256
-__global__ void __launch_bounds__(SELF_THREADS, 2) k_self_periodic(AssembleArgs A, const __grid_constant__ QPLattice L, double3* Fself, int* status)
+// Row `row` (= 4 t + tn) of the periodic domain, by the whole CTA (SELF_THREADS threads).
+__device__ __forceinline__ void self_periodic_row(const AssembleArgs& A, const QPLattice& L, int row, double3* Fself,
+                                                  int* status, double (*red)[24], int* serr)
 {
-  __shared__ double red[SELF_THREADS / 32][24];
-  __shared__ int serr[SELF_THREADS / 32];
-  const int row = blockIdx.x;
   const int t = row >> 2, tn = row & 3;
   SelfInfo S;
   self_setup(A.geo, abs(A.sid[t]), tn, mk(0.0, 0.0), S);
@@ -413,6 +448,13 @@ __global__ void __launch_bounds__(SELF_THREADS, 2) k_self_periodic(AssembleArgs 
   cplx CC[9], dCz[9], dCe[9];
   self_per_combine(S, v, CC, dCz, dCe);
   store_pair(A, row, t, CC, dCz, dCe, Fself, row, -1);
+}
+
+__global__ void __launch_bounds__(SELF_THREADS, 2) k_self_periodic(AssembleArgs A, const __grid_constant__ QPLattice L, double3* Fself, int* status)
+{
+  __shared__ double red[SELF_THREADS / 32][24];
+  __shared__ int serr[SELF_THREADS / 32];
+  self_periodic_row(A, L, blockIdx.x, Fself, status, red, serr);
 }
 
 // ==========================================================================================
@@ -545,7 +587,7 @@ int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, 
         stats->reg_periodic_launches++;
       }
       tic();
-      k_gh_periodic<<<148 * 4, 256, 0, st>>>(A, *L, p0, Fp, gh_list, gh_count, d_status);
+      k_gh_periodic<<<148 * 4, 256, 0, st>>>(A, *L, p0, Fp, gh_list, gh_count, gh_cap, d_status);
       toc(2);
     } else {
       unsigned blocks = (unsigned)((np + 127) / 128);
@@ -553,7 +595,7 @@ int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, 
       k_reg_interior<<<blocks, 128, 0, st>>>(A, p0, np, Fp, gh_list, gh_count, gh_cap, d_status);
       toc(1);
       tic();
-      k_gh_interior<<<148 * 4, 256, 0, st>>>(A, p0, Fp, gh_list, gh_count);
+      k_gh_interior<<<148 * 4, 256, 0, st>>>(A, p0, Fp, gh_list, gh_count, gh_cap);
       toc(2);
     }
     tic();

@@ -8,3 +8,4 @@
 #include "force.cu"
 #include "solve_dtn.cu"
 #include "context.cu"
+#include "batch.cu"

@@ -36,11 +36,11 @@ __device__ void block_sum(double* v, double* red, double* out)
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(SI_THREADS) k_self_interior(AssembleArgs A, double3* Fself)
+// Row `row` (= 4 t + tn) of an interior domain, by the whole CTA (SI_THREADS threads); red, res:
+// its shared reduction buffers.
+__device__ __forceinline__ void self_interior_row(const AssembleArgs& A, int row, double3* Fself, double* red,
+                                                  double (*res)[SELF_NV])
 {
-  __shared__ double red[SI_NW * SELF_NV];
-  __shared__ double res[4][SELF_NV];
-  const int row = blockIdx.x;
   const int t = row >> 2, tn = row & 3;
   const int sd = A.sid[t];
   SelfInfo S;
@@ -86,6 +86,13 @@ __global__ void __launch_bounds__(SI_THREADS) k_self_interior(AssembleArgs A, do
     }
   }
   Fself[row] = make_double3(CC[8].re, dCz[8].re, dCe[8].re);
+}
+
+__global__ void __launch_bounds__(SI_THREADS) k_self_interior(AssembleArgs A, double3* Fself)
+{
+  __shared__ double red[SI_NW * SELF_NV];
+  __shared__ double res[4][SELF_NV];
+  self_interior_row(A, blockIdx.x, Fself, red, res);
 }
 
 void bem3_launch_self_interior(const AssembleArgs& A, double3* Fself, int* d_status, cudaStream_t st)

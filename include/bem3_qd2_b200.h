@@ -237,6 +237,64 @@ int bem3_ctx_field(bem3_ctx c, int n, const double *r, int type, int total, doub
  * Points other than nodes need the quasi-periodic open region (BEM3_ERR_ARG otherwise). */
 int bem3_ctx_force(bem3_ctx c, const double *rc, int type, double *F, double *N);
 
+/* ---------------------------------------------------------------------------------------------
+ * Batched assembly: the coefficient matrices of many domains of many instances (each its own
+ * mesh, wavelength, incidence and lattice) in one launch per pair class, replayed as one CUDA
+ * graph.  No counterpart in the reference (one domain per create_cmatrix_domain call,
+ * d3qd2_solve_bieq.c:165); each domain's results are those of bem3_assemble_domain_dev on the
+ * same inputs.
+ *
+ * One entry per (instance, domain), all pointers device memory on the current device:
+ * geo/Ne and sid/Ne_d/did/periodic as bem3_assemble_domain_dev; qd the instance's lattice and
+ * Bloch wave vector (periodic domains); outputs G, H, dG, dH, dF in the reference layout (dG, dH,
+ * dF may be NULL). */
+typedef struct {
+  const double *geo;
+  int Ne;
+  const int *sid;
+  int Ne_d;
+  int did;
+  int periodic;
+  bem3_qpd2 qd;
+  double kre, kim;
+  double *G, *H, *dG, *dH, *dF;
+} bem3_batch_domain;
+
+/* Launch shape of a batch (bem3_batch_create with NULL takes {8, 2, 4}).
+ *   grab_units          work units (2 regular periodic pairs each) a warp takes per atomic
+ *                       on the batch's work counter, 1..4096
+ *   regp_blocks_per_sm  resident CTAs per SM of the persistent regular periodic kernel, 1..2
+ *   gh_blocks_per_sm    CTAs per SM of the near-singular kernels, 1..16 */
+typedef struct {
+  int grab_units;
+  int regp_blocks_per_sm;
+  int gh_blocks_per_sm;
+} bem3_batch_tuning;
+
+typedef struct bem3_batch_s *bem3_batch;
+
+/* Device bytes bem3_batch_create allocates for these domains (an upper bound): per domain
+ * 96 Ne_d^2 bytes of per-pair F terms, its near-singular work list and self-pair terms, plus the
+ * descriptor table.  The outputs are the caller's. */
+size_t bem3_batch_scratch_bytes(const bem3_batch_domain *doms, int n);
+
+/* Builds a batch over n <= 65535 domains: descriptor table, work segments, scratch (one
+ * cudaMalloc) and the captured graph.  Synchronous.  Must not be called during a stream capture. */
+int bem3_batch_create(const bem3_batch_domain *doms, int n, const bem3_batch_tuning *tune, bem3_batch *out);
+
+/* Enqueues one assembly of every domain of the batch on `stream` (one graph launch).  Runs of
+ * the same batch must not overlap: they share its scratch. */
+int bem3_batch_run(bem3_batch b, void *stream);
+
+/* Waits for `stream` and returns 0 or the first failing domain's status code (kernel codes as
+ * for bem3_assemble_domain_dev); per_domain (optional, n entries) receives every domain's. */
+int bem3_batch_wait(bem3_batch b, void *stream, int *per_domain);
+
+/* Kernels one run launches, and the device bytes the batch holds. */
+int bem3_batch_info(bem3_batch b, int *launches, size_t *device_bytes);
+
+int bem3_batch_destroy(bem3_batch b);
+
 /* Gauss-Legendre nodes and weights on [-1, 1] (the reference's gauleg, com_src/gauleg.c:3). */
 void bem3_gauss_legendre(int n, double *x, double *w);
 

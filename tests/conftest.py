@@ -57,6 +57,13 @@ def gpu_available():
 
 
 @pytest.fixture(scope="session")
+def cuda_lib_host():
+    """The CUDA library loaded without a GPU, for its entry points that touch no device."""
+    import bem3_emf_qd2_b200 as B
+    return B.lib()
+
+
+@pytest.fixture(scope="session")
 def cuda_lib():
     import bem3_emf_qd2_b200 as B
     if not gpu_available():
