@@ -125,6 +125,8 @@ def lib():
         L.bem3_ctx_set_bv.argtypes = [vp, C.POINTER(bem3_bv)]
         L.bem3_ctx_domain_id.argtypes = [vp, i, vp, vp]
         L.bem3_ctx_field.argtypes = [vp, i, vp, i, i, vp, vp, vp]
+        L.bem3_ctx_potential.argtypes = [vp, i, vp, i, i, vp, vp]
+        L.bem3_ctx_field_memp.argtypes = [vp, i, vp, i, i, vp, vp, vp]
         L.bem3_ctx_force.argtypes = [vp, vp, i, vp, vp]
         L.bem3_geo_stride.restype = i
         L.bem3_last_gh_pairs.restype = C.c_ulonglong
@@ -377,15 +379,38 @@ class Context:
         return plane_power(lambda r, total: self.field(r, type_, total), p.vd1, p.vd2, p.waves[0].cos_t > 0,
                            z_top, z_bottom, n)
 
-    def field(self, r, type_: int = 0, total: bool = True):
-        """E, H [n,3] complex and the domain of each point (EH_t if total else EH_s)."""
+    def field(self, r, type_: int = 0, total=True):
+        """E, H [n,3] complex and the domain of each point: EH_t (total True / 1), EH_s (False / 0)
+        or EH_i (2, the incident field alone)."""
         r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
         E = np.zeros((len(r), 3), np.complex128)
         H = np.zeros((len(r), 3), np.complex128)
         did = np.zeros(len(r), np.int32)
-        check(lib().bem3_ctx_field(self.h, len(r), _ptr(r), type_, 1 if total else 0, _ptr(E), _ptr(H), _ptr(did)),
+        check(lib().bem3_ctx_field(self.h, len(r), _ptr(r), type_, int(total), _ptr(E), _ptr(H), _ptr(did)),
               "bem3_ctx_field")
         return E, H, did
+
+    def field_memp(self, r, type_: int = 0, total=True):
+        """E, H [n,3] from the derivatives of the potentials (EH_mEMP_t / _s / _i for total
+        True or 1 / 0 / 2) and the domain of each point (negative where the point is too close
+        to the boundary for these rules)."""
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+        E = np.zeros((len(r), 3), np.complex128)
+        H = np.zeros((len(r), 3), np.complex128)
+        did = np.zeros(len(r), np.int32)
+        check(lib().bem3_ctx_field_memp(self.h, len(r), _ptr(r), type_, int(total), _ptr(E), _ptr(H), _ptr(did)),
+              "bem3_ctx_field_memp")
+        return E, H, did
+
+    def potential(self, r, type_: int = 0, total=True):
+        """Modified electromagnetic potentials U [n,4] complex (vector potential, scalar potential)
+        and the domain of each point: mEMP_t (total True / 1), mEMP_s (0) or mEMP_i (2)."""
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+        U = np.zeros((len(r), 4), np.complex128)
+        did = np.zeros(len(r), np.int32)
+        check(lib().bem3_ctx_potential(self.h, len(r), _ptr(r), type_, int(total), _ptr(U), _ptr(did)),
+              "bem3_ctx_potential")
+        return U, did
 
 
 def solve_bieq(problem: Problem):

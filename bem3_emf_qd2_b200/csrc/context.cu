@@ -641,6 +641,7 @@ FieldArgs field_view(bem3_ctx c)
     A.sid[d] = c->dsid[d].as<int>();
     A.E[d] = c->E[d].as<double>(); A.dE[d] = c->dE[d].as<double>();
     A.H[d] = c->H[d].as<double>(); A.dH[d] = c->dH[d].as<double>();
+    A.U[d] = c->U[d].as<double>(); A.dU[d] = c->dU[d].as<double>();
     A.kn[2 * d] = c->kn[2 * d]; A.kn[2 * d + 1] = c->kn[2 * d + 1];
   }
   A.vk0 = c->qd.vk[0]; A.vk1 = c->qd.vk[1];
@@ -675,9 +676,12 @@ extern "C" int bem3_ctx_domain_id(bem3_ctx c, int n, const double* r, int* did)
   return cudaMemcpy(did, ddid.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : BEM3_ERR_CUDA;
 }
 
-extern "C" int bem3_ctx_field(bem3_ctx c, int n, const double* r, int type, int total, double* E, double* H, int* did)
+// E, H (pot false) or U (pot true) at n points; mode 0 scattered / interior, 1 total, 2 incident.
+static int ctx_field_run(bem3_ctx c, int n, const double* r, int type, int mode, bool pot, double* E, double* H,
+                         int* did)
 {
-  if (!c || n < 0 || (n > 0 && (!r || !E || !H)) || type < 0 || type > 3) return BEM3_ERR_ARG;
+  if (!c || n < 0 || (n > 0 && (!r || !E || (!pot && !H))) || type < 0 || type > 3 || mode < 0 || mode > 2)
+    return BEM3_ERR_ARG;
   if (n == 0) return 0;
   DeviceGuard g(c->dev);
   if (type >= 2 && ensure_tables() != 0) return BEM3_ERR_CUDA;  // Gauss-Legendre tables
@@ -685,10 +689,50 @@ extern "C" int bem3_ctx_field(bem3_ctx c, int n, const double* r, int type, int 
   DevBuf dr, ddid, dcell, dE, dH;
   int rc = run_domain_id(c, A, n, r, dr, ddid, dcell);
   if (rc) return rc;
+  const size_t eo = (size_t)n * (pot ? 8 : 6) * sizeof(double);
+  if (dE.alloc(eo) || (!pot && dH.alloc((size_t)n * 6 * sizeof(double)))) return BEM3_ERR_CUDA;
+  cudaMemset(c->status.p, 0, sizeof(int));
+  if (pot)
+    k_field_t<true><<<(unsigned)n, FIELD_THREADS>>>(A, c->L, n, dr.as<double>(), ddid.as<int>(), dcell.as<int2>(), type,
+                                                    mode, dE.as<double>(), nullptr, c->status.as<int>());
+  else
+    k_field_t<false><<<(unsigned)n, FIELD_THREADS>>>(A, c->L, n, dr.as<double>(), ddid.as<int>(), dcell.as<int2>(), type,
+                                                     mode, dE.as<double>(), dH.as<double>(), c->status.as<int>());
+  if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
+  int hs = 0;
+  if (cudaMemcpy(&hs, c->status.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(E, dE.p, eo, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      (!pot && cudaMemcpy(H, dH.p, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+      (did && cudaMemcpy(did, ddid.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess))
+    return BEM3_ERR_CUDA;
+  return hs;
+}
+
+extern "C" int bem3_ctx_field(bem3_ctx c, int n, const double* r, int type, int total, double* E, double* H, int* did)
+{
+  return ctx_field_run(c, n, r, type, total, false, E, H, did);
+}
+
+extern "C" int bem3_ctx_potential(bem3_ctx c, int n, const double* r, int type, int total, double* U, int* did)
+{
+  return ctx_field_run(c, n, r, type, total, true, U, nullptr, did);
+}
+
+extern "C" int bem3_ctx_field_memp(bem3_ctx c, int n, const double* r, int type, int total, double* E, double* H,
+                                   int* did)
+{
+  if (!c || n < 0 || (n > 0 && (!r || !E || !H)) || type < 0 || type > 3 || total < 0 || total > 2) return BEM3_ERR_ARG;
+  if (n == 0) return 0;
+  DeviceGuard g(c->dev);
+  if (type >= 2 && ensure_tables() != 0) return BEM3_ERR_CUDA;
+  FieldArgs A = field_view(c);
+  DevBuf dr, ddid, dcell, dE, dH;
+  int rc = run_domain_id(c, A, n, r, dr, ddid, dcell);
+  if (rc) return rc;
   if (dE.alloc((size_t)n * 6 * sizeof(double)) || dH.alloc((size_t)n * 6 * sizeof(double))) return BEM3_ERR_CUDA;
   cudaMemset(c->status.p, 0, sizeof(int));
-  k_field<<<(unsigned)n, FIELD_THREADS>>>(A, c->L, n, dr.as<double>(), ddid.as<int>(), dcell.as<int2>(), type,
-                                          total ? 1 : 0, dE.as<double>(), dH.as<double>(), c->status.as<int>());
+  k_eh_memp<<<(unsigned)n, FIELD_THREADS>>>(A, c->L, n, dr.as<double>(), ddid.as<int>(), dcell.as<int2>(), type, total,
+                                            c->lambda0, dE.as<double>(), dH.as<double>(), c->status.as<int>());
   if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
   int hs = 0;
   if (cudaMemcpy(&hs, c->status.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||

@@ -241,6 +241,179 @@ BEM_HD int field_coef(const double* geo, int sd, const double* rt, cplx k, int t
   return err;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Coefficients and their gradients with respect to the point, for the fields computed from the
+// derivatives of the potentials (q0_dcoef_rt_grad d3qd2_elem.c:650-682 and dcoef_rt_grad
+// :316-349: q0_bil_dcoef_grad.c, q0_lit_dcoef_grad.c, bil_dcoef_grad.c, lit_dcoef_grad.c, types
+// 0-3).  dC[p][n] = d CC[n] / d rt_p; dF[p] = dF / d rt_p.  The periodic kernels need the QPGF's
+// second derivatives (qpgf_eval2).
+struct GradKer {
+  cplx g, h, dg[3], dh[3];
+  double tD, dF[3];
+};
+
+// Kernel values at one quadrature point, R = r(point) - rt, W the normal used by the rule:
+// g, h = G and grad G . W; dg, dh their derivatives with respect to R (the rules apply the sign
+// of d/d rt); tD = (R . W) / |R|^3 and its derivative dF.  Free space without the 1/(4 pi).
+template <bool PER>
+BEM_HD int grad_kernel(const QPLattice& L, cplx k, const double* vR, const double* vW, GradKer& o)
+{
+  const double aR = vnorm3(vR);
+  const double i_aR = 1.0 / aR, i3 = i_aR * i_aR * i_aR;
+  const double rdW = dot3(vR, vW) * i_aR;
+  o.tD = rdW * i_aR * i_aR;
+  for (int p = 0; p < 3; p++) o.dF[p] = i3 * (3.0 * vR[p] * i_aR * rdW - vW[p]);
+  if (PER) {
+    QPVal2 v;
+    const int err = qpgf_eval2(L, vR, v);
+    o.g = v.G;
+    o.h = v.dG[0] * vW[0] + v.dG[1] * vW[1] + v.dG[2] * vW[2];
+    const cplx* d2 = v.d2G;  // xx, yy, zz, xy, yz, zx
+    o.dh[0] = d2[0] * vW[0] + d2[3] * vW[1] + d2[5] * vW[2];
+    o.dh[1] = d2[3] * vW[0] + d2[1] * vW[1] + d2[4] * vW[2];
+    o.dh[2] = d2[5] * vW[0] + d2[4] * vW[1] + d2[2] * vW[2];
+    for (int p = 0; p < 3; p++) o.dg[p] = v.dG[p];
+    return err;
+  }
+  const cplx kR = k * aR;
+  const cplx ca = mul_i(kR), cb = ca - mk(1.0, 0.0);
+  const cplx ce = (k.im == 0.0) ? expi(kR.re) : cexp_(ca);
+  o.g = ce * i_aR;
+  o.h = cb * ce * o.tD;
+  const cplx a3 = kR * kR + 3.0 * cb;
+  for (int p = 0; p < 3; p++) {
+    o.dg[p] = cb * ce * (i_aR * i_aR * vR[p] * i_aR);
+    o.dh[p] = ce * i3 * (a3 * (vR[p] * i_aR * rdW) - cb * vW[p]);
+  }
+  return 0;
+}
+
+template <bool PER>
+BEM_HD int field_grad_coef(const double* geo, int sd, const double* rt, cplx k, int type, const QPLattice& L,
+                           const FieldGL* gl, cplx* CC, cplx (*dC)[8], double& F, double* dF)
+{
+  for (int i = 0; i < 8; i++) {
+    CC[i] = mk(0.0, 0.0);
+    for (int p = 0; p < 3; p++) dC[p][i] = mk(0.0, 0.0);
+  }
+  F = 0.0;
+  dF[0] = dF[1] = dF[2] = 0.0;
+  if (PER && sd < 0) return -1;
+  if (type < 0 || type > 3 || (type >= 2 && !gl)) return -1;
+  const int s = sd < 0 ? -sd : sd;
+  const double* g = geo + (size_t)s * GEO_STRIDE;
+  Elem el;
+  load_elem(geo, s, el);
+  const int nn = el.nn;
+  int err = 0;
+  GradKer q;
+  double vR[3], vW[3];
+  // one quadrature point: weight w, shape-function values N (nn of them), area factor aW (quads)
+  auto add = [&](double w, const double* N, double aW) {
+    for (int ep = 0; ep < nn; ep++) {
+      const double wn = w * N[ep];
+      CC[ep] += q.g * (wn * aW);
+      CC[ep + 4] += q.h * wn;
+      for (int p = 0; p < 3; p++) {
+        dC[p][ep] += q.dg[p] * (wn * aW);
+        dC[p][ep + 4] += q.dh[p] * wn;
+      }
+    }
+    F += w * q.tD;
+    for (int p = 0; p < 3; p++) dF[p] += w * q.dF[p];
+  };
+  const int n = (type == 2) ? 12 : 64;
+  const double* x = (type == 2) ? (gl ? gl->x12 : nullptr) : (gl ? gl->x64 : nullptr);
+  const double* wq = (type == 2) ? (gl ? gl->w12 : nullptr) : (gl ? gl->w64 : nullptr);
+  double sG, sH, sdG, sdH, sF;  // end scaling of G, H, dG, dH and F parts
+  if (nn == 4) {
+    if (type == 0) {  // the element's nodes, node weights 1 (q0_bil_dcoef_grad_4p, bil_dcoef_grad_4p)
+      for (int i = 0; i < 4; i++) {
+        for (int l = 0; l < 3; l++) { vR[l] = g[GEO_REN + 3 * i + l] - rt[l]; vW[l] = g[GEO_WEN + 3 * i + l]; }
+        const int st = grad_kernel<PER>(L, k, vR, vW, q);
+        if (st < 0) err = st;
+        double N[4] = {0.0, 0.0, 0.0, 0.0};
+        N[i] = 1.0;
+        add(1.0, N, vnorm3(vW));
+      }
+    } else {
+      const int npts = (type == 1) ? 9 : n * n;
+      for (int i = 0; i < npts; i++) {
+        double z, e, w, N[4];
+        if (type == 1) fq_gauss9(i, z, e, w);
+        else rule_point(4, n, x, wq, i, z, e, w);
+        bil_rw(el, z, e, vR, vW);
+        for (int l = 0; l < 3; l++) vR[l] -= rt[l];
+        const int st = grad_kernel<PER>(L, k, vR, vW, q);
+        if (st < 0) err = st;
+        bil_N4(z, e, N);
+        add(w, N, vnorm3(vW));
+      }
+    }
+    sG = PER ? 1.0 : EL_I_FP;
+    sH = sG;
+    sdG = -sG;
+    sdH = PER ? -1.0 : EL_I_FP;
+    sF = EL_I_FP;
+  } else {
+    // flat triangle: one normal for the whole element -- the node-0 normal (4-point rules, and the
+    // 7-point periodic rule) or W = cw[:, 0] (7-point free-space rule, Gauss-Legendre rules)
+    const bool wen0 = (type == 0) || (type == 1 && PER);
+    for (int l = 0; l < 3; l++) vW[l] = wen0 ? g[GEO_WEN + l] : g[GEO_CW + 3 * l];
+    const double aV = vnorm3(vW);
+    if (type == 0) {  // nodes 0-2 (weight 25/48) and the centroid (weight -27/48, shape functions 1/3)
+      for (int i = 0; i < 4; i++) {
+        for (int l = 0; l < 3; l++) vR[l] = g[GEO_REN + 3 * i + l] - rt[l];
+        const int st = grad_kernel<PER>(L, k, vR, vW, q);
+        if (st < 0) err = st;
+        double N[3] = {0.0, 0.0, 0.0};
+        if (i < 3) N[i] = 1.0;
+        else lit_N3(0.0, 0.0, N);
+        add((i < 3) ? FQ_T4W0 : -FQ_T4W1, N, 1.0);
+      }
+    } else {
+      const int npts = (type == 1) ? 7 : 3 * n * n;
+      for (int i = 0; i < npts; i++) {
+        double z, e, w, N[3];
+        if (type == 1) fq_tri7(i, z, e, w);
+        else rule_point(3, n, x, wq, i, z, e, w);
+        lit_r(el, z, e, vR);
+        for (int l = 0; l < 3; l++) vR[l] -= rt[l];
+        const int st = grad_kernel<PER>(L, k, vR, vW, q);
+        if (st < 0) err = st;
+        lit_N3(z, e, N);
+        add(w, N, 1.0);
+      }
+    }
+    if (type <= 1) {
+      const double c = PER ? 0.5 : FQ_I_EP;
+      sG = c * aV; sH = c; sdG = -c * aV; sdH = PER ? -c : c;
+      sF = FQ_I_EP;
+    } else {
+      const double c = 0.0625 * EL_SQ3 * EL_I_SPSQ3;
+      sG = (PER ? 1.0 / 24.0 : c) * aV; sH = PER ? 1.0 / 24.0 : c;
+      sdG = -sG; sdH = PER ? -1.0 / 24.0 : c;
+      sF = c;
+    }
+  }
+  for (int i = 0; i < 4; i++) {
+    CC[i] = CC[i] * sG;
+    CC[i + 4] = CC[i + 4] * sH;
+    for (int p = 0; p < 3; p++) { dC[p][i] = dC[p][i] * sdG; dC[p][i + 4] = dC[p][i + 4] * sdH; }
+  }
+  F *= sF;
+  for (int p = 0; p < 3; p++) dF[p] *= sF;
+  if (sd < 0) {  // seen from the other side (bil_convert_dCC / lit_convert_dCC, d3qd2_elem.c:938-947)
+    for (int i = 4; i < 8; i++) {
+      CC[i] = -CC[i];
+      for (int p = 0; p < 3; p++) dC[p][i] = -dC[p][i];
+    }
+    F = -F;
+    for (int p = 0; p < 3; p++) dF[p] = -dF[p];
+  }
+  return err;
+}
+
 // Solid angle of a flat triangle (or of a quad split into two triangles along 0-2) seen from the
 // origin, vertices given relative to the point (fid_calc_solid_angle, d3qd2_setup.c:1351-1422):
 // the spherical excess of the triangle of unit vectors, from the angles between the planes

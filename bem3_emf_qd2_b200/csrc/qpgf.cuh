@@ -556,6 +556,266 @@ QP_EVAL_FN int qpgf_eval(const QPLattice& L, const double* r_in, QPVal& out)
   return err;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Second derivatives: G, grad G and the Hessian d2G = (xx, yy, zz, xy, yz, zx) at r, for the fields
+// computed from the derivatives of the potentials (d3hm_qpgf_d2_v2, d3_qpgf_d2.c:178-230 with
+// :321-345, 440-466, 887-1044, 2011-2399).  The method choice, lattice reduction and split
+// parameter are those of qpgf_eval; the terms, their order (rows outward from the centre row,
+// centre term then each side) and the stop rules are the reference's v2 rules: the real-space and
+// Ewald spectral sums stop on d2G_xx and d2G_yy, the Fourier-domain sum on d2G_zz.  A plain form
+// (one term at a time, phases by sincos) for field points; the assembly does not use it.
+struct QPVal2 {
+  cplx G;
+  cplx dG[3];
+  cplx d2G[6];
+};
+
+BEM_HD void qp2_acc(cplx& S, cplx* dS, cplx* d2S, const cplx& F, const cplx* dF, const cplx* d2F)
+{
+  S += F;
+  for (int i = 0; i < 3; i++) dS[i] += dF[i];
+  for (int i = 0; i < 6; i++) d2S[i] += d2F[i];
+}
+
+// Ewald real-space term (d3_qpgf_d2.c:2157-2199); dF[2], d2F[4], d2F[5] still lack the factor z
+// that the sum applies at the end.
+BEM_HD void qp2_ew1_term(const QPLattice& L, const double* r, double veps, int l1, int l2, cplx& F, cplx* dF, cplx* d2F)
+{
+  const double R0 = (double)l1 * L.d1x + (double)l2 * L.d2x;
+  const double R1 = (double)l1 * L.d1y + (double)l2 * L.d2y;
+  const double ra0 = r[0] + R0, ra1 = r[1] + R1, ra2 = r[2];
+  const double rl = sqrt(ra0 * ra0 + ra1 * ra1 + ra2 * ra2);
+  const double i_rl = 1.0 / rl, i_rl2 = i_rl * i_rl;
+  const double ke = L.k * veps, i_ve = 1.0 / veps, rl_2e = rl * 0.5 * i_ve;
+  const cplx cef = expi(L.vkx * R0 + L.vky * R1) * exp(ke * ke - rl_2e * rl_2e);
+  const cplx w = faddeeva_w(ke, rl_2e);
+  const cplx cf1 = cef * (i_rl2 * (i_rl * w.re - L.k * w.im + i_ve * QP_INV_SQRTPI));
+  const cplx cf2 = cef * (i_rl2 * (L.k * L.k * i_rl * 2.0 * w.re - i_ve * i_ve * i_ve * QP_INV_SQRTPI));
+  const cplx cf3 = cf1 * (-6.0 * i_rl2) + cf2;
+  F = cef * (i_rl * w.re);
+  dF[0] = cf1 * ra0; dF[1] = cf1 * ra1; dF[2] = cf1;
+  d2F[0] = 2.0 * cf1 + cf3 * (ra0 * ra0);
+  d2F[1] = 2.0 * cf1 + cf3 * (ra1 * ra1);
+  d2F[2] = 2.0 * cf1 + cf3 * (ra2 * ra2);
+  d2F[3] = cf3 * (ra0 * ra1);
+  d2F[4] = cf3 * ra1;
+  d2F[5] = cf3 * ra0;
+}
+
+// Ewald spectral term (d3_qpgf_d2.c:2343-2399): 0 propagating, 1 evanescent, -3 beta_n == 0.
+BEM_HD int qp2_ew2_term(const QPLattice& L, const double* r, double veps, int n1, int n2, cplx& F, cplx* dF, cplx* d2F)
+{
+  const double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
+  const double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
+  const double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
+  const cplx ce = expi(an0 * r[0] + an1 * r[1]);
+  const double azve = r[2] / (2.0 * veps);
+  const double ef = exp(bn2 * veps * veps - azve * azve);
+  const double c2 = 2.0 * QP_INV_SQRTPI / veps * ef;
+  int e;
+  cplx Fc, Gc, d2z;
+  if (bn2 > 0.0) {
+    const double bn = sqrt(bn2);
+    const cplx ff = expi(bn * r[2]);
+    const cplx w = faddeeva_w(bn * veps, azve);
+    Fc = mk(2.0 * ff.re, 2.0 * (ef * w.im + ff.im));   // 2 (i ef Im w + ff)
+    Gc = mk(2.0 * (ef * w.re - ff.re), -2.0 * ff.im);  // 2 (ef Re w - ff)
+    F = (ce * (1.0 / bn)) * Fc;
+    d2z = mul_i(Fc) * bn + mk(c2, 0.0);
+    e = 0;
+  } else if (bn2 < 0.0) {
+    const double bn = sqrt(-bn2);
+    const double ebz = exp(bn * r[2]);
+    const double f1 = ebz * erfc(bn * veps + azve), f2 = erfc(bn * veps - azve) / ebz;
+    Fc = mk(f1 + f2, 0.0);
+    Gc = mk(f1 - f2, 0.0);
+    F = mul_mi(ce * ((f1 + f2) / bn));
+    d2z = mk(-bn * (f1 + f2) + c2, 0.0);
+    e = 1;
+  } else {
+    return -3;
+  }
+  dF[0] = F * an0; dF[1] = F * an1; dF[2] = ce * Gc;
+  d2F[0] = dF[0] * an0; d2F[1] = dF[1] * an1; d2F[2] = ce * d2z;
+  d2F[3] = dF[0] * an1; d2F[4] = dF[2] * an1; d2F[5] = dF[2] * an0;
+  return e;
+}
+
+// Fourier-domain term (d3_qpgf_d2.c:1010-1044): 0 propagating, 1 evanescent, -2 beta_n == 0.
+BEM_HD int qp2_fd_term(const QPLattice& L, const double* r, int n1, int n2, cplx& F, cplx* dF, cplx* d2F)
+{
+  const double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
+  const double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
+  const double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
+  int e;
+  if (bn2 > 0.0) {
+    const double bn = sqrt(bn2);
+    dF[2] = expi(an0 * r[0] + an1 * r[1] + bn * fabs(r[2]));
+    F = dF[2] * (1.0 / bn);
+    e = 0;
+  } else if (bn2 < 0.0) {
+    const double bn = sqrt(-bn2);
+    dF[2] = expi(an0 * r[0] + an1 * r[1]) * exp(-bn * fabs(r[2]));
+    F = mul_mi(dF[2] * (1.0 / bn));
+    e = 1;
+  } else {
+    return -2;
+  }
+  dF[0] = F * an0; dF[1] = F * an1;
+  d2F[0] = dF[0] * an0; d2F[1] = dF[1] * an1; d2F[2] = F * bn2;
+  d2F[3] = dF[1] * an0; d2F[4] = dF[2] * an1; d2F[5] = dF[2] * an0;
+  return e;
+}
+
+// Ewald real-space sum (d3_qpgf_d2.c:2053-2155).  Returns the number of terms or -1.
+BEM_HD int qp2_ew1_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS, cplx* d2S)
+{
+  S = mk(0, 0);
+  for (int i = 0; i < 3; i++) dS[i] = mk(0, 0);
+  for (int i = 0; i < 6; i++) d2S[i] = mk(0, 0);
+  int cc = 0;
+  cplx F, dF[3], d2F[6];
+  for (int dir = 0; dir < 3; dir++) {
+    const int step = (dir == 2) ? -1 : 1;
+    int l1 = (dir == 0) ? 0 : step;
+    for (;; l1 += step) {
+      if (dir != 0 && (l1 >= QP_EW_LIMIT || l1 <= -QP_EW_LIMIT)) return -1;
+      const cplx o0 = d2S[0], o1 = d2S[1];
+      const int lc = -(int)round(((r[0] + (double)l1 * L.d1x) * L.d2x + (r[1] + (double)l1 * L.d1y) * L.d2y) / L.ad22);
+      qp2_ew1_term(L, r, veps, l1, lc, F, dF, d2F);
+      qp2_acc(S, dS, d2S, F, dF, d2F);
+      cc++;
+      for (int side = 1; side >= -1; side -= 2) {
+        int off = 1;
+        for (; off < QP_EW_LIMIT; off++) {
+          qp2_ew1_term(L, r, veps, l1, lc + side * off, F, dF, d2F);
+          qp2_acc(S, dS, d2S, F, dF, d2F);
+          cc++;
+          if (qp_diff(d2F[0], d2S[0], eps) && qp_diff(d2F[1], d2S[1], eps)) break;
+        }
+        if (off == QP_EW_LIMIT) return -1;
+      }
+      if (dir == 0) break;
+      if (qp_comp(d2S[0], o0, eps) && qp_comp(d2S[1], o1, eps)) break;
+    }
+  }
+  const double f4p = 4.0 * QP_PI, f8p = 8.0 * QP_PI;
+  S = S * (1.0 / f4p);
+  dS[0] = dS[0] * (-1.0 / f4p); dS[1] = dS[1] * (-1.0 / f4p); dS[2] = dS[2] * (-r[2] / f4p);
+  for (int i = 0; i < 4; i++) d2S[i] = d2S[i] * (-1.0 / f8p);
+  d2S[4] = d2S[4] * (-r[2] / f8p); d2S[5] = d2S[5] * (-r[2] / f8p);
+  return cc;
+}
+
+// Spectral sums.  FD == 0: Ewald spectral (d3_qpgf_d2.c:2201-2341; returns terms or -2 / -3);
+// FD == 1: Fourier domain (d3_qpgf_d2.c:887-1008; terms or -1 / -2 / -4).
+template <int FD>
+BEM_HD int qp2_spec_sum(const QPLattice& L, const double* r, double veps, double eps, cplx& S, cplx* dS, cplx* d2S)
+{
+  if (FD && r[2] == 0.0) return -4;
+  const int LIMIT = FD ? QP_FD_LIMIT : QP_EW_LIMIT;
+  const int ELIM = FD ? -1 : -2;
+  S = mk(0, 0);
+  for (int i = 0; i < 3; i++) dS[i] = mk(0, 0);
+  for (int i = 0; i < 6; i++) d2S[i] = mk(0, 0);
+  const int nc = L.nc1;
+  int cc = 0;
+  cplx F, dF[3], d2F[6];
+  for (int dir = 0; dir < 3; dir++) {
+    const int step = (dir == 2) ? -1 : 1;
+    int n1 = nc + ((dir == 0) ? 0 : step);
+    for (;; n1 += step) {
+      if (dir != 0 && (n1 - nc >= LIMIT || n1 - nc <= -LIMIT)) return ELIM;
+      const cplx o0 = d2S[0], o1 = d2S[1], o2 = d2S[2];
+      int nc2;
+      if (FD) nc2 = (int)round((L.vkx * L.g2x + L.vky * L.g2y - (double)n1 * L.g12) / L.g22);
+      else nc2 = (int)round(-((-L.vkx + (double)n1 * L.g1x) * L.g2x + (-L.vky + (double)n1 * L.g1y) * L.g2y) / L.g22);
+      int e = FD ? qp2_fd_term(L, r, n1, nc2, F, dF, d2F) : qp2_ew2_term(L, r, veps, n1, nc2, F, dF, d2F);
+      if (e < 0) return e;
+      qp2_acc(S, dS, d2S, F, dF, d2F);
+      cc++;
+      int flg = 0;
+      for (int side = 1; side >= -1; side -= 2) {
+        int off = 1;
+        for (; off < LIMIT; off++) {
+          e = FD ? qp2_fd_term(L, r, n1, nc2 + side * off, F, dF, d2F)
+                 : qp2_ew2_term(L, r, veps, n1, nc2 + side * off, F, dF, d2F);
+          if (e < 0) return e;
+          qp2_acc(S, dS, d2S, F, dF, d2F);
+          cc++;
+          if (e > 0) {
+            if (FD ? qp_diff(d2F[2], d2S[2], eps) : (qp_diff(d2F[0], d2S[0], eps) && qp_diff(d2F[1], d2S[1], eps))) break;
+          } else {
+            flg++;
+          }
+        }
+        if (off == LIMIT) return ELIM;
+      }
+      if (dir == 0) break;
+      if (FD) {
+        if (qp_comp(d2S[2], o2, eps)) break;
+      } else if (flg == 0 && qp_comp(d2S[0], o0, eps) && qp_comp(d2S[1], o1, eps)) {
+        break;
+      }
+    }
+  }
+  const double aidd = fabs(L.idd);
+  if (FD) {
+    const double sgnz = r[2] / fabs(r[2]), c = 0.5 * aidd;
+    S = mul_i(S * c);
+    dS[0] = dS[0] * -c; dS[1] = dS[1] * -c; dS[2] = dS[2] * (-c * sgnz);
+    for (int i = 0; i < 4; i++) d2S[i] = mul_i(d2S[i] * -c);
+    d2S[4] = mul_i(d2S[4] * (-c * sgnz)); d2S[5] = mul_i(d2S[5] * (-c * sgnz));
+  } else {
+    const double cd = 0.25 * aidd;
+    S = mul_i(S * cd);
+    dS[0] = dS[0] * -cd; dS[1] = dS[1] * -cd; dS[2] = dS[2] * cd;
+    d2S[0] = mul_i(d2S[0] * -cd); d2S[1] = mul_i(d2S[1] * -cd); d2S[2] = d2S[2] * -cd;
+    d2S[3] = mul_i(d2S[3] * -cd); d2S[4] = mul_i(d2S[4] * cd); d2S[5] = mul_i(d2S[5] * cd);
+  }
+  return cc;
+}
+
+// G, grad G and d2G at r_in.  Return value as d3hm_qpgf_d2_v2: > 0 terms; -11..-14 FD errors,
+// -21..-24 EW errors.
+BEM_HD int qpgf_eval2(const QPLattice& L, const double* r_in, QPVal2& out)
+{
+  const double eps = QP_MEPS;
+  const int l1 = (int)floor((r_in[0] * L.d2y - r_in[1] * L.d2x) * L.idd + 0.5);
+  const int l2 = (int)floor(-(r_in[0] * L.d1y - r_in[1] * L.d1x) * L.idd + 0.5);
+  double r[3];
+  r[0] = r_in[0] - (double)l1 * L.d1x - (double)l2 * L.d2x;
+  r[1] = r_in[1] - (double)l1 * L.d1y - (double)l2 * L.d2y;
+  r[2] = r_in[2];
+  bool use_fd = false;
+  if (!L.ew_only)
+    use_fd = (L.bN / L.bNp * exp(-L.bNp * fabs(r[2])) < eps) && (L.bN / L.bNm * exp(-L.bNm * fabs(r[2])) < eps);
+  int err;
+  if (use_fd) {
+    err = qp2_spec_sum<1>(L, r, 0.0, eps, out.G, out.dG, out.d2G);
+    if (err < 0) return err - 10;
+  } else {
+    double veps = L.veps0;
+    const double r2_min = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    if (L.k * L.k * veps * veps - r2_min / (4.0 * veps * veps) > QP_EW_EXPM)
+      veps = sqrt(QP_EW_EXPM + sqrt(L.k * L.k * r2_min + QP_EW_EXPM * QP_EW_EXPM)) / (sqrt(2.0) * L.k);
+    const int c1 = qp2_ew1_sum(L, r, veps, eps, out.G, out.dG, out.d2G);
+    if (c1 < 0) return c1 - 20;
+    cplx S2, dS2[3], d2S2[6];
+    const int c2 = qp2_spec_sum<0>(L, r, veps, eps, S2, dS2, d2S2);
+    if (c2 < 0) return c2 - 20;
+    qp2_acc(out.G, out.dG, out.d2G, S2, dS2, d2S2);
+    err = c1 + c2;
+  }
+  if (l1 != 0 || l2 != 0) {
+    const cplx cf = expi(-(L.vkx * ((double)l1 * L.d1x + (double)l2 * L.d2x) + L.vky * ((double)l1 * L.d1y + (double)l2 * L.d2y)));
+    out.G = out.G * cf;
+    for (int i = 0; i < 3; i++) out.dG[i] = out.dG[i] * cf;
+    for (int i = 0; i < 6; i++) out.d2G[i] = out.d2G[i] * cf;
+  }
+  return err;
+}
+
 // Lattice constants, following d3_qpgf_d2.c:129-155 (selection), :1680-1685 (split parameter)
 // and :1848-1857 (reciprocal vectors) expression by expression.
 BEM_HD int qp_lattice_init(QPLattice& L, double k, double vkx, double vky, double d1x, double d1y, double d2x, double d2y)

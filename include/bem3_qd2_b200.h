@@ -221,14 +221,30 @@ int bem3_ctx_set_bv(bem3_ctx c, const bem3_bv *bv /* [MN+1] */);
 /* Domain of each point (q0_domain_id / domain_id, d3qd2_setup.c:157-238): did[n]. */
 int bem3_ctx_domain_id(bem3_ctx c, int n, const double *r, int *did);
 
-/* Electromagnetic field at n points (EH_s / EH_t, d3qd2_src/d3qd2_field.c:203-285).
+/* Electromagnetic field at n points (EH_s / EH_t / EH_i, d3qd2_src/d3qd2_field.c:203-300).
  * r: [n][3]; E, H: [n][3] complex; did: [n] domain of each point (may be NULL).
  * type 0: nodal 4-point rules, type 1: 9-point (quads) / 7-point (triangles) rules, types 2 and
  * 3: 12 x 12 and 64 x 64 Gauss-Legendre rules (three sub-quads on triangles), for points near the
  * boundary.  (The reference's type 4, double-exponential integration, is not provided.)
- * total != 0 adds the incident field in the open region (EH_t), else scattered/internal (EH_s).
- * Points outside every domain get did = -1 and zero fields. */
+ * total 0: scattered / internal field (EH_s); 1: plus the incident field in the open region
+ * (EH_t); 2: the incident field alone, at every point (EH_i).
+ * Points outside every domain get did = -1 and zero fields (except with total 2). */
 int bem3_ctx_field(bem3_ctx c, int n, const double *r, int type, int total, double *E, double *H, int *did);
+
+/* Modified electromagnetic potentials at n points (mEMP_s / mEMP_t / mEMP_i,
+ * d3qd2_src/d3qd2_field.c:10-87): U [n][4] complex = (vector potential x, y, z, scalar
+ * potential).  type, total and did as bem3_ctx_field; total 1 adds the incident electric field
+ * to the vector potential in the open region, total 2 gives U = (E_inc, 0). */
+int bem3_ctx_potential(bem3_ctx c, int n, const double *r, int type, int total, double *U, int *did);
+
+/* Electromagnetic field at n points from the derivatives of the potentials (EH_mEMP_s / _t / _i,
+ * d3qd2_src/d3qd2_field.c:89-201): E = A - grad phi, H = lambda0 / (2 pi i) curl A, with the
+ * coefficient-gradient rules (q0_dcoef_rt_grad / dcoef_rt_grad, d3qd2_elem.c:316, 650) and the
+ * Green's function's second derivatives (d3hm_qpgf_d2_v2).  More accurate than bem3_ctx_field in
+ * the far field, slower.  type and total as bem3_ctx_field.  A point too close to the boundary
+ * for these rules (|dF/dr| > 10, CBD_CDF) gets zero fields and did = -did (-99 in the open
+ * region), as the reference returns. */
+int bem3_ctx_field_memp(bem3_ctx c, int n, const double *r, int type, int total, double *E, double *H, int *did);
 
 /* Radiation force F[3] and torque N[3] about rc[3] on the objects, from the Maxwell stress tensor
  * of the total field on the open region's boundary (force_FN, d3qd2_src/d3qd2_force.c:10-54).

@@ -258,6 +258,19 @@ void rp_qpgf_dqG(int n, const double *r, const double *p, double eps, double com
   for (i = 0; i < n; i++) ret[i] = d3hm_qpgf_d2_dqG(out + 3 * (size_t)i, (double *)r + 3 * (size_t)i, eps, &q);
 }
 
+/* d3hm_qpgf_d2_v2 (d3_qpgf_d2.c:178-230): out per point qG, dqG[3], d2qG[6] (xx, yy, zz, xy,
+ * yz, zx). */
+void rp_qpgf_v2(int n, const double *r, const double *p, double eps, double complex *out, int *ret)
+{
+  QPD2 q;
+  int i;
+  set_qpd(&q, p);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (i = 0; i < n; i++)
+    ret[i] = d3hm_qpgf_d2_v2(out + 10 * (size_t)i, out + 10 * (size_t)i + 1, out + 10 * (size_t)i + 4,
+                             (double *)r + 3 * (size_t)i, eps, &q);
+}
+
 void rp_faddeeva(int n, const double complex *z, double relerr, double complex *w)
 {
   int i;
@@ -309,19 +322,65 @@ void rp_set_bv(int d, const double complex *U, const double complex *dU, const d
 }
 
 /* EH_t / EH_s at n points (d3qd2_field.c:203,271); returns domain ids in did. */
+/* total: 0 EH_s, 1 EH_t, 2 EH_i (d3qd2_field.c:203-300) */
 void rp_EH(int n, const double *r, int type, int total, double complex *E, double complex *H, int *did)
 {
   int i;
 #pragma omp parallel for schedule(dynamic)
   for (i = 0; i < n; i++) {
-    if (total) did[i] = EH_t(E + 3 * (size_t)i, H + 3 * (size_t)i, (double *)r + 3 * (size_t)i, type, &g_qd);
-    else did[i] = EH_s(E + 3 * (size_t)i, H + 3 * (size_t)i, (double *)r + 3 * (size_t)i, type, &g_qd);
+    double complex *e = E + 3 * (size_t)i, *h = H + 3 * (size_t)i;
+    double *p = (double *)r + 3 * (size_t)i;
+    if (total == 2) did[i] = EH_i(e, h, p, type, &g_qd);
+    else if (total) did[i] = EH_t(e, h, p, type, &g_qd);
+    else did[i] = EH_s(e, h, p, type, &g_qd);
+  }
+}
+
+/* Modified electromagnetic potentials U[4] (vector potential, scalar potential) at points;
+ * total: 0 mEMP_s, 1 mEMP_t, 2 mEMP_i (d3qd2_field.c:10-87). */
+void rp_mEMP(int n, const double *r, int type, int total, double complex *U, int *did)
+{
+  int i;
+#pragma omp parallel for schedule(dynamic)
+  for (i = 0; i < n; i++) {
+    double complex *u = U + 4 * (size_t)i;
+    double *p = (double *)r + 3 * (size_t)i;
+    if (total == 2) did[i] = mEMP_i(u, p, type, &g_qd);
+    else if (total) did[i] = mEMP_t(u, p, type, &g_qd);
+    else did[i] = mEMP_s(u, p, type, &g_qd);
+  }
+}
+
+/* Fields from the derivatives of the potentials; total: 0 EH_mEMP_s, 1 EH_mEMP_t, 2 EH_mEMP_i
+ * (d3qd2_field.c:89-201). */
+void rp_EH_mEMP(int n, const double *r, int type, int total, double complex *E, double complex *H, int *did)
+{
+  int i;
+#pragma omp parallel for schedule(dynamic)
+  for (i = 0; i < n; i++) {
+    double complex *e = E + 3 * (size_t)i, *h = H + 3 * (size_t)i;
+    double *p = (double *)r + 3 * (size_t)i;
+    if (total == 2) did[i] = EH_mEMP_i(e, h, p, type, &g_qd);
+    else if (total) did[i] = EH_mEMP_t(e, h, p, type, &g_qd);
+    else did[i] = EH_mEMP_s(e, h, p, type, &g_qd);
   }
 }
 
 int rp_force(double *F, double *N, const double *rc, int type) { return force_FN(F, N, (double *)rc, type, &g_qd); }
 
 int rp_domain_id(const double *r) { return q0_domain_id((double *)r, &g_qd); }
+
+/* Coefficients and their gradients of source element sd at point rt for domain did, as
+ * EH_mEMP_s (d3qd2_field.c:124-125) computes them: CC[9], dC[3][9]. */
+void rp_dcoef_rt_grad(int did, const double *rt, int sd, int type, double complex *CC, double complex *dC)
+{
+  double complex d[3][9];
+  int p, i;
+  if (did == 0 && g_qd.bd.ps == 1) q0_dcoef_rt_grad(CC, d, (double *)rt, sd, g_qd.kn[did], type, &(g_qd.bd));
+  else dcoef_rt_grad(CC, d, (double *)rt, sd, g_qd.kn[did], type, &(g_qd.bd));
+  for (p = 0; p < 3; p++)
+    for (i = 0; i < 9; i++) dC[9 * p + i] = d[p][i];
+}
 
 /* Field coefficients of source element sd (signed id) at point rt for domain did, as EH_s
  * (d3qd2_field.c:229-231) computes them: q0_coef_rt in the periodic open region, coef_rt else. */

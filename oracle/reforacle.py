@@ -73,11 +73,15 @@ class RefOracle:
         lib.rp_assemble_rows.argtypes = [C.c_int, C.c_int, C.c_int, _cp, _cp, _cp, _cp, _dp, C.c_int]
         for f in (lib.rp_qpgf_v1, lib.rp_qpgf_qG, lib.rp_qpgf_dqG):
             f.argtypes = [C.c_int, _dp, _dp, C.c_double, _cp, _ip]
+        lib.rp_dcoef_rt_grad.argtypes = [C.c_int, _dp, C.c_int, C.c_int, _cp, _cp]
+        lib.rp_qpgf_v2.argtypes = [C.c_int, _dp, _dp, C.c_double, _cp, _ip]
         lib.rp_faddeeva.argtypes = [C.c_int, _cp, C.c_double, _cp]
         lib.rp_coef_rt.argtypes = [C.c_int, _dp, C.c_int, C.c_int, _cp]
         lib.rp_get_bv.argtypes = [C.c_int, _cp, _cp, _cp, _cp, _cp, _cp]
         lib.rp_set_bv.argtypes = [C.c_int, _cp, _cp, _cp, _cp, _cp, _cp]
         lib.rp_EH.argtypes = [C.c_int, _dp, C.c_int, C.c_int, _cp, _cp, _ip]
+        lib.rp_mEMP.argtypes = [C.c_int, _dp, C.c_int, C.c_int, _cp, _ip]
+        lib.rp_EH_mEMP.argtypes = [C.c_int, _dp, C.c_int, C.c_int, _cp, _cp, _ip]
         lib.rp_force.argtypes = [_dp, _dp, _dp, C.c_int]
         lib.rp_force.restype = C.c_int
         lib.rp_domain_id.argtypes = [_dp]
@@ -163,6 +167,9 @@ class RefOracle:
         if kind == "v1":
             out = np.zeros((n, 4), np.complex128)
             self.lib.rp_qpgf_v1(n, r, qpd, eps, out, ret)
+        elif kind == "v2":
+            out = np.zeros((n, 10), np.complex128)
+            self.lib.rp_qpgf_v2(n, r, qpd, eps, out, ret)
         elif kind == "qG":
             out = np.zeros((n, 1), np.complex128)
             self.lib.rp_qpgf_qG(n, r, qpd, eps, out, ret)
@@ -198,11 +205,28 @@ class RefOracle:
         a = {k: np.ascontiguousarray(v, dtype=np.complex128) for k, v in bv.items()}
         self.lib.rp_set_bv(d, a["U"], a["dU"], a["E"], a["dE"], a["H"], a["dH"])
 
-    def EH(self, r: np.ndarray, type_: int = 0, total: bool = True):
+    def EH(self, r: np.ndarray, type_: int = 0, total=True):
+        """EH_s (total 0 / False), EH_t (1 / True) or EH_i (2) at points."""
         r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
         E = np.zeros((len(r), 3), np.complex128); H = np.zeros_like(E)
         did = np.zeros(len(r), np.int32)
         self.lib.rp_EH(len(r), r, type_, int(total), E, H, did)
+        return E, H, did
+
+    def mEMP(self, r: np.ndarray, type_: int = 0, total=True):
+        """mEMP_s / mEMP_t / mEMP_i (total 0, 1, 2): U[4] = (vector potential, scalar potential)."""
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+        U = np.zeros((len(r), 4), np.complex128)
+        did = np.zeros(len(r), np.int32)
+        self.lib.rp_mEMP(len(r), r, type_, int(total), U, did)
+        return U, did
+
+    def EH_mEMP(self, r: np.ndarray, type_: int = 0, total=True):
+        """EH_mEMP_s / _t / _i (total 0, 1, 2): fields from the potentials' derivatives."""
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1, 3)
+        E = np.zeros((len(r), 3), np.complex128); H = np.zeros_like(E)
+        did = np.zeros(len(r), np.int32)
+        self.lib.rp_EH_mEMP(len(r), r, type_, int(total), E, H, did)
         return E, H, did
 
     def force(self, rc=(0.0, 0.0, 0.0), type_: int = 0):
@@ -215,6 +239,13 @@ class RefOracle:
         out = np.zeros(9, np.complex128)
         self.lib.rp_coef_rt(did, np.ascontiguousarray(r, np.float64), sd, type_, out)
         return out
+
+    def dcoef_rt_grad(self, did: int, r, sd: int, type_: int):
+        """CC[9] and dC[3][9] of source element sd at point r (EH_mEMP_s's per-element values)."""
+        cc = np.zeros(9, np.complex128)
+        dc = np.zeros(27, np.complex128)
+        self.lib.rp_dcoef_rt_grad(did, np.ascontiguousarray(r, np.float64), sd, type_, cc, dc)
+        return cc, dc.reshape(3, 9)
 
     def domain_id(self, r) -> int:
         return int(self.lib.rp_domain_id(np.asarray(r, np.float64)))

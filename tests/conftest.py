@@ -37,11 +37,13 @@ def devmath_host():
     lib.hm_faddeeva.argtypes = [i, vp, vp]
     lib.hm_faddeeva_fast.argtypes = [i, vp, vp]
     lib.hm_qpgf.argtypes = [i, vp, vp, i, vp, vp]
+    lib.hm_qpgf2.argtypes = [i, vp, vp, vp, vp]
     lib.hm_pair_regular.argtypes = [vp, i, i, i, i, d, d, vp, i, vp, vp, vp]
     lib.hm_pair_regular.restype = i
     lib.hm_self_interior.argtypes = [vp, i, i, d, d, vp, vp, vp, vp, vp]
     lib.hm_self_periodic.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp]
     lib.hm_field_coef.argtypes = [vp, i, vp, i, d, d, i, vp, vp, vp]
+    lib.hm_field_grad_coef.argtypes = [vp, i, vp, i, d, d, i, vp, vp, vp]
     lib.hm_solid_angle.argtypes = [vp, vp, i, i, vp, vp]
     lib.hm_solid_angle.restype = d
     lib.hm_self_periodic.restype = i

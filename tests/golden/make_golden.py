@@ -6,7 +6,7 @@ from its sources by oracle/Makefile and called through oracle/reforacle.py:
 
   gauleg.npz    the Gauss-Legendre tables of gauleg (com_src/gauleg.c) for n = 12, 64
   faddeeva.npz  Faddeeva_w (qgf2_src/Faddeeva.cc) at seeded points, relerr 1e-15
-  qpgf.npz      d3hm_qpgf_d2_v1 / _qG / _dqG (qgf2_src/d3_qpgf_d2.c) for 5 lattices
+  qpgf.npz      d3hm_qpgf_d2_v1 / _qG / _dqG / _v2 (qgf2_src/d3_qpgf_d2.c) for 5 lattices
   rows_*.npz    inputs of a sample problem shipped with the reference (read by the reference's
                 own readers) and complete rows of create_cmatrix_domain
                 (d3qd2_src/d3qd2_solve_bieq.c:165-256) for selected collocation elements.
@@ -16,11 +16,13 @@ from its sources by oracle/Makefile and called through oracle/reforacle.py:
                 force_FN (d3qd2_force.c) for those results, types 0 and 1.
   near_fields.npz  the reference's EH_t, types 0-3, at points just off the boundary of those
                 results.
+  potentials.npz  the reference's mEMP_s/_t/_i (types 0-3), EH_i and EH_mEMP_s/_t/_i (types
+                0-2) at the probe points and the near-boundary points of those results.
   power.npz     incident, reflected and transmitted power through one unit cell for those
                 results, from the reference's EH_t / EH_s on two planes.
 
 Usage: python tests/golden/make_golden.py [reference_dir] [section ...]
-       sections: gauleg faddeeva qpgf rows bv near power (default: all)
+       sections: gauleg faddeeva qpgf rows bv near potentials power (default: all)
 """
 import os
 import sys
@@ -37,7 +39,7 @@ from bem3_emf_qd2_b200.dqd2 import load_inputs  # noqa: E402
 
 REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 SECTIONS = {a for a in sys.argv[2:] if "=" not in a} or {"gauleg", "faddeeva", "qpgf", "rows", "bv", "near",
-                                                         "power"}
+                                                         "potentials", "power"}
 ONLY = {x for a in sys.argv[2:] if a.startswith("only=") for x in a[5:].split(",")}
 
 
@@ -144,6 +146,32 @@ def near_fields(o):
     np.savez_compressed(os.path.join(HERE, "near_fields.npz"), **out)
 
 
+def potentials(o):
+    """The reference's modified potentials (mEMP_s / _t / _i, types 0-3), incident field (EH_i) and
+    fields from the potentials' derivatives (EH_mEMP_s / _t / _i, types 0-2) at the probe points of
+    each shipped result file and at points just off its boundary (near_fields.npz)."""
+    near = np.load(os.path.join(HERE, "near_fields.npz"))
+    out = {}
+    for name, (sub, dat, msh, rot, pts) in BV_CASES.items():
+        o.load_dat(os.path.join(REF, sub, dat))
+        r = np.concatenate([np.array(pts, float), near[name + "/r"]])
+        out[name + "/r"] = r
+        for ty in (0, 1, 2, 3):
+            for mode in (0, 1, 2):
+                U, did = o.mEMP(r, ty, mode)
+                out[f"{name}/U{ty}_{mode}"] = U
+                out[f"{name}/did"] = did
+        E, H, _ = o.EH(r, 0, 2)
+        out[name + "/Ei"], out[name + "/Hi"] = E, H
+        for ty in (0, 1, 2):
+            for mode in (0, 1, 2):
+                E, H, did = o.EH_mEMP(r, ty, mode)
+                out[f"{name}/mE{ty}_{mode}"], out[f"{name}/mH{ty}_{mode}"] = E, H
+                out[f"{name}/mdid{ty}_{mode}"] = did
+        print(name, "potentials done", flush=True)
+    np.savez_compressed(os.path.join(HERE, "potentials.npz"), **out)
+
+
 POWER = {"veri": (1.4, -1.4, 16), "ex2": (1.2, -1.2, 16)}  # z_top, z_bottom, grid
 
 
@@ -177,6 +205,8 @@ def main():
         power_balance(o)
     if "near" in SECTIONS:
         near_fields(o)
+    if "potentials" in SECTIONS:
+        potentials(o)
     if "gauleg" in SECTIONS:
         gauleg_tables(o)
     if "bv" in SECTIONS:
@@ -202,6 +232,9 @@ def main():
         v1, rv1 = o.qpgf(r, p, "v1")
         g, rg = o.qpgf(r, p, "qG")
         d, rd = o.qpgf(r, p, "dqG")
+        v2, rv2 = o.qpgf(r, p, "v2")
+        out[name + "/v2"] = v2
+        out[name + "/ret_v2"] = rv2
         out[name + "/qpd"] = p
         out[name + "/r"] = r
         out[name + "/v1"] = v1

@@ -14,6 +14,22 @@ void hm_faddeeva(int n, const double* z, double* w)
   }
 }
 
+// Second derivatives: out = qG, dqG[3], d2qG[6] interleaved re/im (20 doubles per point)
+void hm_qpgf2(int n, const double* r, const double* p, double* out, int* ret)
+{
+  QPLattice L;
+  qp_lattice_init(L, p[0], p[1], p[2], p[4], p[5], p[6], p[7]);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < n; i++) {
+    QPVal2 v;
+    ret[i] = qpgf_eval2(L, r + 3 * i, v);
+    double* o = out + 20 * (size_t)i;
+    o[0] = v.G.re; o[1] = v.G.im;
+    for (int c = 0; c < 3; c++) { o[2 + 2 * c] = v.dG[c].re; o[3 + 2 * c] = v.dG[c].im; }
+    for (int c = 0; c < 6; c++) { o[8 + 2 * c] = v.d2G[c].re; o[9 + 2 * c] = v.d2G[c].im; }
+  }
+}
+
 // p = k, vk[3], vd1[2], vd2[2] (the reference's QPD2 order); out = qG, dqG[3] interleaved re/im
 void hm_qpgf(int n, const double* r, const double* p, int mode, double* out, int* ret)
 {
@@ -161,6 +177,25 @@ int hm_field_coef(const double* geo, int sd, const double* rt, int periodic, dou
                     : field_coef<false>(geo, sd, rt, mk(kre, kim), type, L, CC, F, &tabs);
   for (int i = 0; i < 8; i++) { out[2 * i] = CC[i].re; out[2 * i + 1] = CC[i].im; }
   out[16] = F;
+  return st;
+}
+
+// field_grad_coef: out = CC[8], dC[3][8] (re/im pairs, 64 doubles), F, dF[3]
+int hm_field_grad_coef(const double* geo, int sd, const double* rt, int periodic, double kre, double kim, int type,
+                       const double* p, const double* gl, double* out)
+{
+  QPLattice L;
+  qp_lattice_init(L, p[0], p[1], p[2], p[4], p[5], p[6], p[7]);
+  const FieldGL tabs = {gl, gl + 12, gl + 24, gl + 88};
+  cplx CC[8], dC[3][8];
+  double F, dF[3];
+  int st = periodic ? field_grad_coef<true>(geo, sd, rt, mk(kre, kim), type, L, &tabs, CC, dC, F, dF)
+                    : field_grad_coef<false>(geo, sd, rt, mk(kre, kim), type, L, &tabs, CC, dC, F, dF);
+  for (int i = 0; i < 8; i++) { out[2 * i] = CC[i].re; out[2 * i + 1] = CC[i].im; }
+  for (int q = 0; q < 3; q++)
+    for (int i = 0; i < 8; i++) { out[16 + 16 * q + 2 * i] = dC[q][i].re; out[17 + 16 * q + 2 * i] = dC[q][i].im; }
+  out[64] = F;
+  for (int q = 0; q < 3; q++) out[65 + q] = dF[q];
   return st;
 }
 

@@ -66,6 +66,41 @@ def test_field_coefficients_match_reference(devmath_host, tmp_path, name):
                     assert abs(out[16] - ref[8].real) <= 1e-12 * max(abs(ref[8].real), 1e-3), (name, did, sd, ty)
 
 
+@pytest.mark.skipif(not HAVE_REF, reason="reference oracle not built in this checkout")
+@pytest.mark.parametrize("name", ["sphere96", "cone210"])
+def test_coefficient_gradients_match_reference(devmath_host, tmp_path, name):
+    """field_grad_coef (the rules of the far-field path) against the reference's q0_dcoef_rt_grad
+    / dcoef_rt_grad, element by element: CC, dC/drt, F and dF/drt to 1e-11 of each part's
+    largest entry (the QPGF's second derivatives agree with d3hm_qpgf_d2_v2 term for term)."""
+    o, p = _setup(name, tmp_path)
+    geo = _packed(p)
+    q = p.qpd
+    qp = np.array([q["k"], *q["vk"], *q["vd1"], *q["vd2"]], np.float64)
+    pts = np.array([[0.05, -0.02, 0.6], [0.3, 0.2, -0.45], [0.01, 0.03, 0.02]])
+    gl = golden("gauleg.npz")
+    tabs = np.ascontiguousarray(np.concatenate([gl["x12"], gl["w12"], gl["x64"], gl["w64"]]))
+    for r in pts:
+        for did in range(p.MN + 1):
+            periodic = 1 if (did == 0 and p.ps == 1) else 0
+            k = complex(p.kn[did])
+            for sd in p.sid[did][::5]:
+                for ty in ((0, 1, 2, 3) if sd == p.sid[did][0] else (0, 1, 2)):
+                    cc, dc = o.dcoef_rt_grad(did, r, int(sd), ty)
+                    out = np.zeros(68)
+                    st = devmath_host.hm_field_grad_coef(geo.ctypes.data, int(sd), r.ctypes.data, periodic, k.real,
+                                                         k.imag, ty, qp.ctypes.data, tabs.ctypes.data,
+                                                         out.ctypes.data)
+                    assert st >= 0
+                    got_cc = out[0:16:2] + 1j * out[1:16:2]
+                    got_dc = (out[16:64:2] + 1j * out[17:64:2]).reshape(3, 8)
+                    what = (name, did, int(sd), ty)
+                    assert np.abs(got_cc - cc[:8]).max() <= 1e-11 * np.abs(cc[:8]).max(), what
+                    assert np.abs(got_dc - dc[:, :8]).max() <= 1e-11 * np.abs(dc[:, :8]).max(), what
+                    assert abs(out[64] - cc[8].real) <= 1e-11 * max(abs(cc[8].real), 1e-3), what
+                    sf = max(np.abs(dc[:, 8].real).max(), 1e-3)
+                    assert np.abs(out[65:68] - dc[:, 8].real).max() <= 1e-11 * sf, what
+
+
 @pytest.mark.parametrize("name", ["sphere96", "cone210"])
 def test_solid_angles_sum_to_the_enclosed_domain(devmath_host, tmp_path, name):
     """Over a closed surface the element solid angles add to 4 pi inside and 0 outside."""

@@ -66,6 +66,26 @@ def test_qpgf_host_build(devmath_host, mode):
         assert np.max(np.abs(got - ref) / scale) < 1e-10, n
 
 
+def test_qpgf_second_derivatives_host_build(devmath_host):
+    """qpgf_eval2 (the header code the field kernels run) against the reference's
+    d3hm_qpgf_d2_v2: the same term counts at every point and G, grad G, d2G to 1e-10 of each
+    point's largest component of that order."""
+    q = golden("qpgf.npz")
+    names = sorted({k.split("/")[0] for k in q.files})
+    for n in names:
+        r = np.ascontiguousarray(q[n + "/r"])
+        out = np.zeros(len(r) * 20)
+        ret = np.zeros(len(r), np.int32)
+        devmath_host.hm_qpgf2(len(r), r.ctypes.data, np.ascontiguousarray(q[n + "/qpd"]).ctypes.data,
+                              out.ctypes.data, ret.ctypes.data)
+        got = (out[0::2] + 1j * out[1::2]).reshape(-1, 10)
+        ref = q[n + "/v2"]
+        assert np.array_equal(ret, q[n + "/ret_v2"]), n
+        for lo, hi in ((0, 1), (1, 4), (4, 10)):
+            scale = np.abs(ref[:, lo:hi]).max(axis=1, keepdims=True)
+            assert np.max(np.abs(got[:, lo:hi] - ref[:, lo:hi]) / scale) < 1e-10, (n, lo)
+
+
 def _pack(p):
     geo = np.zeros((p.Ne + 1, 48))
     geo[:, 0:12] = p.cr.reshape(-1, 12)
