@@ -21,6 +21,13 @@
 //    Algorithm 916, 2011.)
 //  * Im z < 0: reflection w(z) = 2 exp(-z^2) - w(-z).
 // The weights e^{-t_n^2} below were computed with mpmath at 40 digits for h = 0.42.
+//
+// The assembly kernels' form (FAST) replaces the series and the trapezoidal rule (|z| < 8) by
+// Weideman's rational approximation (SIAM J. Numer. Anal. 31 (1994) 1497-1518), a polynomial of
+// degree 39 in Z = (L + iz)/(L - iz) times 1/(L - iz)^2 plus pi^{-1/2}/(L - iz): one complex
+// reciprocal and 39 complex multiply-adds, no branch inside the disk (coefficients in
+// faddeeva_weideman.h, generated by gen_faddeeva_weideman.py), and the continued fraction in its
+// single-division (Wallis) form for |z| >= 8.
 #pragma once
 
 #include "cplx.cuh"
@@ -30,6 +37,8 @@
 #else
 #define BEM_CONST static const
 #endif
+
+#include "faddeeva_weideman.h"
 
 #define FAD_NFULL 18
 #define FAD_NHALF 17
@@ -94,6 +103,19 @@ template <bool FAST>
 BEM_HD_NOINLINE cplx faddeeva_w_upper_t(double x, double y)
 {
   const double r2 = x * x + y * y;
+  if (FAST && r2 < 64.0) {
+    BEM_STAT_W(1);
+    const cplx il = crecip_fast(mk(FAD_WL + y, -x));  // 1 / (L - i z); |L - i z| >= L
+    const cplx Z = mk(FAD_WL - y, x) * il;           // (L + i z) / (L - i z)
+    double pr = fad_wc[0], pi = 0.0;
+#pragma unroll
+    for (int n = 1; n < FAD_WN; n++) {
+      const double t = pr * Z.re - pi * Z.im + fad_wc[n];
+      pi = pr * Z.im + pi * Z.re;
+      pr = t;
+    }
+    return (mk(2.0 * pr, 2.0 * pi) * il + mk(FAD_INV_SQRTPI, 0.0)) * il;
+  }
   if (FAST && r2 >= 64.0 && r2 < 1.0e8) {
     BEM_STAT_W(0);
     // the same 20-level continued fraction by the forward (Wallis) recurrence of its numerators
