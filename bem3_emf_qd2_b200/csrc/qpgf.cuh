@@ -160,16 +160,21 @@ BEM_HD void qp_ew2_prop(const double* r, double veps, double an0, double an1, do
                         cplx* dF)
 {
   BEM_STAT_T(1);
-  double azve = r[2] / (2.0 * veps);
+  // FAST: the term is even in z and its z derivative odd (with ef w(x - iy) = 2 conj(ff) -
+  // ef conj(w(x + iy)), x = bn veps, y = z / (2 veps)), so it is evaluated at |z| in the upper half
+  // plane, without the reflection's extra exponential, and dF[2] takes the sign of z
+  const double zz = FAST ? fabs(r[2]) : r[2];
+  double azve = zz / (2.0 * veps);
   double ef = exp(bn2 * veps * veps - azve * azve);
-  cplx ff = expi(bn * r[2]);
-  cplx w = faddeeva_w_t<FAST>(bn * veps, azve);
+  cplx ff = expi(bn * zz);
+  cplx w = FAST ? faddeeva_w_upper_t<FAST>(bn * veps, azve) : faddeeva_w_t<FAST>(bn * veps, azve);
   // Fn = 2 ce / bn (i ef Im w + ff)
   cplx t = mk(ff.re, ef * w.im + ff.im);
   F = FAST ? (ce * (2.0 / bn)) * t : mk(2.0 * ce.re / bn, 2.0 * ce.im / bn) * t;
   dF[0] = F * an0;
   dF[1] = F * an1;
   dF[2] = 2.0 * (ce * mk(ef * w.re - ff.re, -ff.im));
+  if (FAST && r[2] < 0.0) dF[2] = -dF[2];
 }
 // ibn = 1/bn: the evaluation forms below differ only in how they obtain bn and 1/bn.
 // FAST: with a = bn veps and b = z / (2 veps) (so that bn z = 2 a b),
