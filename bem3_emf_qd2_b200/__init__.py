@@ -192,19 +192,38 @@ class MeshArrays:
         return geo
 
 
-def assemble_domain(problem: Problem, did: int, derivatives: bool = True):
+def domain_outputs(problem: Problem, did: int, derivatives: bool = True, pinned: bool = False) -> dict:
+    """Host arrays for assemble_domain's outputs (page-locked when `pinned`, through torch, so that
+    the library's row-chunk copies run asynchronously)."""
+    N = 4 * len(problem.sid[did])
+    shapes = dict(G=(N, N), H=(N, N), dF=(N, 3))
+    if derivatives:
+        shapes.update(dG=(2 * N, N), dH=(2 * N, N))
+    out = {}
+    for k, shp in shapes.items():
+        dt = np.float64 if k == "dF" else np.complex128
+        if pinned:
+            import torch
+            t = torch.empty(shp, dtype=torch.float64 if k == "dF" else torch.complex128, pin_memory=True)
+            out[k] = t.numpy()
+            out["_" + k] = t  # keeps the page-locked allocation alive
+        else:
+            out[k] = np.zeros(shp, dt)
+    if not derivatives:
+        out["dG"] = out["dH"] = None
+    return out
+
+
+def assemble_domain(problem: Problem, did: int, derivatives: bool = True, out: dict = None):
     """Coefficient matrices of domain `did` on the GPU (host in, host out).
 
     Returns dict G, H [N,N], dG, dH [2N,N] (complex), dF [N,3] with N = 4 Ne_d, in the layout of
-    the reference's temp files (d3qd2_solve_bieq.c:213-236)."""
+    the reference's temp files (d3qd2_solve_bieq.c:213-236).  `out` (from domain_outputs) supplies
+    the arrays to fill instead of new ones."""
     sid = np.ascontiguousarray(problem.sid[did], dtype=np.int32)
     ne = len(sid)
-    N = 4 * ne
-    G = np.zeros((N, N), np.complex128)
-    H = np.zeros((N, N), np.complex128)
-    dG = np.zeros((2 * N, N), np.complex128) if derivatives else None
-    dH = np.zeros((2 * N, N), np.complex128) if derivatives else None
-    dF = np.zeros((N, 3))
+    o = out if out is not None else domain_outputs(problem, did, derivatives)
+    G, H, dG, dH, dF = o["G"], o["H"], o["dG"], o["dH"], o["dF"]
     ma = MeshArrays(problem)
     q = make_qpd(problem.qpd)
     periodic = 1 if (did == 0 and problem.ps == 1) else 0

@@ -523,8 +523,14 @@ size_t bem3_scratch_bytes(int ne, int rows)
 
 // Runs the whole domain on `stream` using caller-provided scratch (see bem3_scratch_bytes).
 // Returns 0, or a negative code (see bem3_qd2_b200.h).
+// Adds a chunk's near-singular count to the domain's total (no host round trip per chunk).
+__global__ void k_acc_count(const unsigned* __restrict__ cnt, unsigned long long* __restrict__ total)
+{
+  *total += *cnt;
+}
+
 int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, size_t scratch_bytes, int rows_per_chunk,
-                      int* d_status, cudaStream_t st, AssembleStats* stats)
+                      int* d_status, cudaStream_t st, AssembleStats* stats, const ChunkHook* hook)
 {
   if (ensure_tables() != 0) return BEM3_ERR_CUDA;
   const int ne = A.ne;
@@ -534,7 +540,8 @@ int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, 
   char* base = (char*)scratch;
   double3* Fself = (double3*)base;
   size_t off = ((size_t)nrows * sizeof(double3) + 255) & ~(size_t)255;
-  unsigned* gh_count = (unsigned*)(base + off);
+  unsigned* gh_count = (unsigned*)(base + off);               // this chunk's list length
+  unsigned long long* gh_total = (unsigned long long*)(base + off + 8);  // the domain's total
   off += 256;
   double3* Fp = (double3*)(base + off);
   off += (((size_t)rows_per_chunk * ne * sizeof(double3)) + 255) & ~(size_t)255;
@@ -548,6 +555,7 @@ int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, 
   if (A.dH && cudaMemsetAsync(A.dH, 0, 2 * N * N * 16, st) != cudaSuccess) return BEM3_ERR_CUDA;
   if (A.dF && cudaMemsetAsync(A.dF, 0, N * 3 * sizeof(double), st) != cudaSuccess) return BEM3_ERR_CUDA;
   cudaMemsetAsync(Fself, 0, N * sizeof(double3), st);
+  cudaMemsetAsync(gh_total, 0, sizeof(unsigned long long), st);
 
   int launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -601,16 +609,15 @@ int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, 
     tic();
     k_rowsum<<<(nr * 32 + 255) / 256, 256, 0, st>>>(A, r0, nr, Fp, Fself);
     toc(3);
-    launches += 3;
-    if (stats) {
-      unsigned c = 0;
-      cudaMemcpyAsync(&c, gh_count, sizeof c, cudaMemcpyDeviceToHost, st);
-      cudaStreamSynchronize(st);
-      stats->gh_pairs += c;
-    }
+    k_acc_count<<<1, 1, 0, st>>>(gh_count, gh_total);
+    launches += 4;
+    if (hook) hook->fn(hook->user, r0, nr, st);
   }
   if (timing) { cudaEventDestroy(ev0); cudaEventDestroy(ev1); }
-  if (stats) stats->launches += launches;
+  if (stats) {
+    stats->launches += launches;
+    stats->d_gh_total = gh_total;
+  }
   if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
   return 0;
 }

@@ -30,9 +30,17 @@ struct AssembleStats {
   double reg_periodic_ms;        // out: summed duration of k_reg_periodic launches
   int reg_periodic_launches;     // out: number of k_reg_periodic launches
   double class_ms[4];            // out: self, regular, near-singular, row-sum kernels (any domain)
+  unsigned long long* d_gh_total;  // out: device counter of near-singular pairs (read it after the stream syncs)
+};
+
+// Called after each row chunk's kernels are enqueued on `st` (rows r0 .. r0 + nr - 1 are final
+// once they have run): lets a caller copy finished rows out while later chunks compute.
+struct ChunkHook {
+  void (*fn)(void* user, int r0, int nr, cudaStream_t st);
+  void* user;
 };
 
 size_t bem3_scratch_bytes(int ne, int rows);
 int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, size_t scratch_bytes, int rows_per_chunk,
-                      int* d_status, cudaStream_t st, AssembleStats* stats);
+                      int* d_status, cudaStream_t st, AssembleStats* stats, const ChunkHook* hook = nullptr);
 void bem3_launch_self_interior(const AssembleArgs& A, double3* Fself, int* d_status, cudaStream_t st);

@@ -171,9 +171,19 @@ static int default_rows_per_chunk(int ne)
   return (int)rows;
 }
 
-extern "C" int bem3_assemble_domain_dev(const double* geo_dev, int Ne, const int* sid_dev, int Ne_d, int did, int periodic,
-                                        const bem3_qpd2* qd, double kre, double kim, double* G_dev, double* H_dev,
-                                        double* dG_dev, double* dH_dev, double* dF_dev, void* stream)
+// One domain's assembly in flight on a stream: its per-thread resources and counters.
+struct DomainRun {
+  DevRes* R = nullptr;
+  AssembleStats S;
+  bool profiling = false;
+};
+
+// Enqueues the assembly of one domain on `st` (device inputs and outputs) without waiting for it;
+// `hook` (optional) sees every row chunk as its kernels are enqueued.
+static int enqueue_domain(const double* geo_dev, int Ne, const int* sid_dev, int Ne_d, int did, int periodic,
+                          const bem3_qpd2* qd, double kre, double kim, double* G_dev, double* H_dev, double* dG_dev,
+                          double* dH_dev, double* dF_dev, cudaStream_t st, int rows, const ChunkHook* hook,
+                          DomainRun& run)
 {
   if (!geo_dev || !sid_dev || Ne <= 0 || Ne_d <= 0 || Ne_d > 2 * Ne || !G_dev || !H_dev) return BEM3_ERR_ARG;
   QPLattice L;
@@ -182,8 +192,6 @@ extern "C" int bem3_assemble_domain_dev(const double* geo_dev, int Ne, const int
     int e = lattice_from(qd, &L);
     if (e) return e;
   }
-  cudaStream_t st = (cudaStream_t)stream;
-  int rows = default_rows_per_chunk(Ne_d);
   size_t need = bem3_scratch_bytes(Ne_d, rows);
   DevRes* R = nullptr;
   int e = ensure_scratch(need, &R);
@@ -198,31 +206,79 @@ extern "C" int bem3_assemble_domain_dev(const double* geo_dev, int Ne, const int
   }
   if (cudaMemsetAsync(R->status, 0, sizeof(int), st) != cudaSuccess) return BEM3_ERR_CUDA;
   A.terms = nullptr;
-  if (t_profiling) {
+  run.profiling = t_profiling != 0;
+  if (run.profiling) {
     if (!R->terms && cudaMalloc(&R->terms, sizeof(unsigned long long)) != cudaSuccess) return BEM3_ERR_CUDA;
     A.terms = R->terms;
     cudaMemsetAsync(R->terms, 0, sizeof(unsigned long long), st);
   }
-  AssembleStats S;
-  memset(&S, 0, sizeof S);
-  S.time_kernels = t_profiling;
-  e = bem3_assemble_run(A, &L, R->scratch, R->scratch_bytes, rows, R->status, st, &S);
-  if (e) return e;
+  memset(&run.S, 0, sizeof run.S);
+  run.S.time_kernels = t_profiling;
+  run.R = R;
+  return bem3_assemble_run(A, &L, R->scratch, R->scratch_bytes, rows, R->status, st, &run.S, hook);
+}
+
+// Waits for `st` and returns the kernels' status; fills this thread's counters.
+static int finish_domain(cudaStream_t st, const DomainRun& run)
+{
   int hs = 0;
-  unsigned long long terms = 0;
-  if (cudaMemcpyAsync(&hs, R->status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return BEM3_ERR_CUDA;
-  if (A.terms && cudaMemcpyAsync(&terms, A.terms, sizeof terms, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+  unsigned long long terms = 0, gh = 0;
+  if (cudaMemcpyAsync(&hs, run.R->status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return BEM3_ERR_CUDA;
+  if (run.profiling && cudaMemcpyAsync(&terms, run.R->terms, sizeof terms, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return BEM3_ERR_CUDA;
+  if (cudaMemcpyAsync(&gh, run.S.d_gh_total, sizeof gh, cudaMemcpyDeviceToHost, st) != cudaSuccess) return BEM3_ERR_CUDA;
   if (cudaStreamSynchronize(st) != cudaSuccess) return BEM3_ERR_CUDA;
   memset(&t_last_stats, 0, sizeof t_last_stats);
-  t_last_stats.gh_pairs = S.gh_pairs;
+  t_last_stats.gh_pairs = gh;
   t_last_stats.qpgf_terms = terms;
-  t_last_stats.launches = S.launches;
-  t_last_stats.reg_periodic_launches = S.reg_periodic_launches;
-  t_last_stats.reg_periodic_ms = S.reg_periodic_ms;
-  for (int i = 0; i < 4; i++) t_last_stats.class_ms[i] = S.class_ms[i];
+  t_last_stats.launches = run.S.launches;
+  t_last_stats.reg_periodic_launches = run.S.reg_periodic_launches;
+  t_last_stats.reg_periodic_ms = run.S.reg_periodic_ms;
+  for (int i = 0; i < 4; i++) t_last_stats.class_ms[i] = run.S.class_ms[i];
   return hs;
 }
+
+extern "C" int bem3_assemble_domain_dev(const double* geo_dev, int Ne, const int* sid_dev, int Ne_d, int did, int periodic,
+                                        const bem3_qpd2* qd, double kre, double kim, double* G_dev, double* H_dev,
+                                        double* dG_dev, double* dH_dev, double* dF_dev, void* stream)
+{
+  cudaStream_t st = (cudaStream_t)stream;
+  DomainRun run;
+  int e = enqueue_domain(geo_dev, Ne, sid_dev, Ne_d, did, periodic, qd, kre, kim, G_dev, H_dev, dG_dev, dH_dev, dF_dev,
+                         st, default_rows_per_chunk(Ne_d), nullptr, run);
+  if (e) return e;
+  return finish_domain(st, run);
+}
+
+namespace {
+// Row chunks finished on the device, copied to the caller's host matrices on a copy stream as soon
+// as each chunk's kernels have run: the transfer of chunk c overlaps the computation of the chunks
+// after it.  (To page-locked host memory the copies are asynchronous; to pageable memory each copy
+// call returns once done, while the GPU keeps computing the chunks already enqueued.)
+struct RowCopies {
+  size_t N = 0;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> r0, nr;
+  bool failed = false;
+  static void hook(void* user, int r0, int nr, cudaStream_t st)
+  {
+    RowCopies& c = *(RowCopies*)user;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess || cudaEventRecord(e, st) != cudaSuccess) {
+      c.failed = true;
+      if (e) cudaEventDestroy(e);
+      return;
+    }
+    c.ev.push_back(e);
+    c.r0.push_back(r0);
+    c.nr.push_back(nr);
+  }
+  ~RowCopies()
+  {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  }
+};
+}  // namespace
 
 extern "C" int bem3_assemble_domain(const bem3_mesh* mesh, const int* sid, int Ne_d, int did, int periodic,
                                     const bem3_qpd2* qd, double kre, double kim, double* G, double* H, double* dG,
@@ -238,7 +294,17 @@ extern "C" int bem3_assemble_domain(const bem3_mesh* mesh, const int* sid, int N
   const size_t N = (size_t)4 * Ne_d;
   double *dgeo = nullptr, *dG_ = nullptr, *dH_ = nullptr, *ddG = nullptr, *ddH = nullptr, *ddF = nullptr;
   int* dsid = nullptr;
+  cudaStream_t cs = nullptr;
   int rc = BEM3_ERR_CUDA;
+  RowCopies rcp;
+  rcp.N = N;
+  const ChunkHook hook = {RowCopies::hook, &rcp};
+  // about 8 row chunks per domain (at least 64 rows each), so that copies overlap the kernels
+  int rows = (int)((N + 7) / 8);
+  rows = rows < 64 ? 64 : rows;
+  rows = rows > default_rows_per_chunk(Ne_d) ? default_rows_per_chunk(Ne_d) : rows;
+  DomainRun run;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) { cs = nullptr; goto done; }
   if (cudaMalloc(&dgeo, geo.size() * sizeof(double)) != cudaSuccess) goto done;
   if (cudaMalloc(&dsid, Ne_d * sizeof(int)) != cudaSuccess) goto done;
   if (cudaMalloc(&dG_, N * N * 16) != cudaSuccess) goto done;
@@ -248,16 +314,28 @@ extern "C" int bem3_assemble_domain(const bem3_mesh* mesh, const int* sid, int N
   if (dF && cudaMalloc(&ddF, 3 * N * sizeof(double)) != cudaSuccess) goto done;
   if (cudaMemcpy(dgeo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) goto done;
   if (cudaMemcpy(dsid, sid, Ne_d * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) goto done;
-  rc = bem3_assemble_domain_dev(dgeo, Ne, dsid, Ne_d, did, periodic, qd, kre, kim, dG_, dH_, ddG, ddH, ddF, nullptr);
+  rc = enqueue_domain(dgeo, Ne, dsid, Ne_d, did, periodic, qd, kre, kim, dG_, dH_, ddG, ddH, ddF, nullptr, rows, &hook,
+                      run);
   if (rc) goto done;
   rc = BEM3_ERR_CUDA;
-  if (cudaMemcpy(G, dG_, N * N * 16, cudaMemcpyDeviceToHost) != cudaSuccess) goto done;
-  if (cudaMemcpy(H, dH_, N * N * 16, cudaMemcpyDeviceToHost) != cudaSuccess) goto done;
-  if (dG && cudaMemcpy(dG, ddG, 2 * N * N * 16, cudaMemcpyDeviceToHost) != cudaSuccess) goto done;
-  if (dH && cudaMemcpy(dH, ddH, 2 * N * N * 16, cudaMemcpyDeviceToHost) != cudaSuccess) goto done;
-  if (dF && cudaMemcpy(dF, ddF, 3 * N * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) goto done;
-  rc = 0;
+  if (rcp.failed) goto done;
+  for (size_t c = 0; c < rcp.ev.size(); c++) {
+    const size_t a = (size_t)rcp.r0[c], n = (size_t)rcp.nr[c];
+    if (cudaStreamWaitEvent(cs, rcp.ev[c], 0) != cudaSuccess) goto done;
+    if (cudaMemcpyAsync(G + 2 * a * N, dG_ + 2 * a * N, n * N * 16, cudaMemcpyDeviceToHost, cs) != cudaSuccess) goto done;
+    if (cudaMemcpyAsync(H + 2 * a * N, dH_ + 2 * a * N, n * N * 16, cudaMemcpyDeviceToHost, cs) != cudaSuccess) goto done;
+    if (dG && cudaMemcpyAsync(dG + 4 * a * N, ddG + 4 * a * N, 2 * n * N * 16, cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+      goto done;
+    if (dH && cudaMemcpyAsync(dH + 4 * a * N, ddH + 4 * a * N, 2 * n * N * 16, cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+      goto done;
+    if (dF && cudaMemcpyAsync(dF + 3 * a, ddF + 3 * a, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+      goto done;
+  }
+  if (cudaStreamSynchronize(cs) != cudaSuccess) goto done;
+  rc = finish_domain(nullptr, run);
 done:
+  if (cs) { cudaStreamSynchronize(cs); cudaStreamDestroy(cs); }
+  cudaDeviceSynchronize();  // nothing of this call may still use the buffers freed below
   cudaFree(dgeo); cudaFree(dsid); cudaFree(dG_); cudaFree(dH_); cudaFree(ddG); cudaFree(ddH); cudaFree(ddF);
   return rc;
 }
