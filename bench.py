@@ -195,6 +195,29 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def ranks_timed(step, steps, warmup, dist, timer, device="cpu"):
+    """W untimed steps, a barrier, then K timed steps on every rank; returns the time in ms, the
+    maximum over ranks (the slowest rank bounds the whole job).  `timer(fn)` runs fn and returns
+    its duration in ms (CUDA events on the GPU)."""
+    import torch
+    for _ in range(warmup):
+        step()
+    if dist:
+        dist.barrier()
+    ms = timer(lambda: [step() for _ in range(steps)])
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def whole_job_value(pairs_per_step, steps, world, ms):
+    """Pairs per second of the whole job: every rank assembles its own instance."""
+    return pairs_per_step * steps * world / (ms * 1e-3)
+
+
 def run_ours(args):
     import torch
     import bem3_emf_qd2_b200 as B
@@ -225,29 +248,23 @@ def run_ours(args):
         for d in domains:
             dev.assemble(d, sptr)
 
+    def cuda_timer(fn):
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1)
+
     for _ in range(args.warmup):
         step()
-    clocks = ClockSampler(os.path.join(tmp, "clocks.csv"))
+    clocks = ClockSampler(os.path.join(tmp, "clocks.csv"))  # samples the timed steps only
     clocks.start()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1)
+    ms = ranks_timed(step, args.steps, 0, dist, cuda_timer, device="cuda")
     clk = clocks.stop(local)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = pairs * args.steps * world / (ms * 1e-3)
+    value = whole_job_value(pairs, args.steps, world, ms)
 
     # kernel launches per step and the roofline of the dominant kernel (profiling pass, not timed above)
     B.set_profiling(True)
