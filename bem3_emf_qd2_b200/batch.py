@@ -360,7 +360,8 @@ def run_mix(problems, budget: int, tune: bool = True, sequential: bool = True, d
     t_seq = 0.0
     launches = 0
     bad = []
-    for cls, w in waves:
+    import sys
+    for iw, (cls, w) in enumerate(waves):
         insts = [InstanceDevice(problems[i], device) for i in w]
         b = Batch(insts, tunings.get(cls))
         b.run()                     # warm-up (first graph launch loads modules)
@@ -383,6 +384,8 @@ def run_mix(problems, budget: int, tune: bool = True, sequential: bool = True, d
             e1.record()
             torch.cuda.synchronize()
             t_seq += e0.elapsed_time(e1) * 1e-3
+        print(f"wave {iw + 1}/{len(waves)} ({cls}, {len(w)} instances): batched {t_batched:.1f} s, "
+              f"one domain at a time {t_seq:.1f} s so far", file=sys.stderr, flush=True)
         del insts
         torch.cuda.empty_cache()
     pairs = _pairs(problems)
