@@ -255,10 +255,13 @@ class Batch:
         return n.value, b.value
 
     def close(self) -> None:
+        """Frees the batch's scratch and drops its references to the instances (whose matrices the
+        caller may then release)."""
         from . import lib
         if self.h:
             lib().bem3_batch_destroy(self.h)
             self.h = C.c_void_p()
+        self.instances = []
 
     def __del__(self):
         try:
@@ -376,11 +379,13 @@ def run_mix(problems, budget: int, tune: bool = True, sequential: bool = True, d
         bad += [(w, s) for s in st if s]
         launches += b.info()[0]
         b.close()
+        del b
         if sequential:
             torch.cuda.synchronize()
             e0.record()
             for inst in insts:
                 inst.assemble_sequential()
+            del inst
             e1.record()
             torch.cuda.synchronize()
             t_seq += e0.elapsed_time(e1) * 1e-3

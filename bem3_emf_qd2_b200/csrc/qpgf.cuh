@@ -124,8 +124,14 @@ BEM_HD double qp_exp(double x) { return exp(x); }
 // Ewald real-space term (d3_qpgf_d2.c:1814-1838).  F and dF[3] (dF[2] still lacks the
 // factor -z/(4 pi) that the sum applies at the end).  ce = e^{i k||.R_l} is supplied by the
 // caller, which advances it along a row by one complex multiply per term instead of a sincos.
+// FAST: smag and dmag[3] are the running sums' magnitudes (max of |re|, |im|) of S and dS[0..2].
+// Where e^{k^2 eps^2 - R^2 / 4 eps^2} makes the term and its gradient smaller than 3e-13 of them
+// (and |z| >= 3.3), w comes from the asymptotic series (faddeeva_w_asym, relative error below
+// 2e-4): the error it adds is below 5e-17 of each running sum.  Most real-space terms are of this
+// kind; each row side needs one of them for its stop rule.
 template <bool FAST = false>
-BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1, int l2, cplx ce, cplx& F, cplx* dF)
+BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1, int l2, cplx ce, cplx& F, cplx* dF,
+                        double smag = 0.0, const double* dmag = nullptr)
 {
   BEM_STAT_T(0);
   double Rl0 = (double)l1 * L.d1x + (double)l2 * L.d2x;
@@ -144,7 +150,17 @@ BEM_HD void qp_ew1_term(const QPLattice& L, const double* r, double veps, int l1
   double i_ve = 1.0 / veps;
   double rl_2e = rl * 0.5 * i_ve;
   double ef = qp_exp(ke * ke - rl_2e * rl_2e);
-  cplx w = faddeeva_w_t<FAST>(ke, rl_2e);
+  cplx w;
+  const double z2 = ke * ke + rl_2e * rl_2e;
+  bool small = false;
+  if (FAST && dmag && z2 >= 10.9) {
+    const double b = i_rl * ef * 0.6 * rsqrt_(z2);  // bound of |F| (|w| < 0.6 / |z| there)
+    const double bd = b * i_rl * (i_rl + L.k);       // of the w-dependent part of |dF| / |p|
+    small = b <= 3e-13 * smag && fabs(px) * bd <= 3e-13 * dmag[0] && fabs(py) * bd <= 3e-13 * dmag[1] &&
+            bd <= 3e-13 * dmag[2];
+  }
+  if (small) w = faddeeva_w_asym(ke, rl_2e);
+  else w = faddeeva_w_t<FAST>(ke, rl_2e);
   double cfr = i_rl * i_rl * ef * (i_rl * w.re - L.k * w.im + i_ve * QP_INV_SQRTPI);
   cplx cf = ce * cfr;
   F = ce * (i_rl * ef * w.re);
@@ -308,7 +324,13 @@ BEM_HD int qp_ew1_sum_body(const QPLattice& L, const double* r, double veps, dou
   for (;;) {
     const int l2 = lc + (side == 1 ? -off : off);
     cplx F, dF[3];
-    qp_ew1_term<OPT>(L, r, veps, l1, l2, ce, F, dF);
+    if (OPT) {
+      const double dmag[3] = {fmax(fabs(dS[0].re), fabs(dS[0].im)), fmax(fabs(dS[1].re), fabs(dS[1].im)),
+                              fmax(fabs(dS[2].re), fabs(dS[2].im))};
+      qp_ew1_term<OPT>(L, r, veps, l1, l2, ce, F, dF, fmax(fabs(S.re), fabs(S.im)), dmag);
+    } else {
+      qp_ew1_term<OPT>(L, r, veps, l1, l2, ce, F, dF);
+    }
     S += F; dS[0] += dF[0]; dS[1] += dF[1]; dS[2] += dF[2];
     cc++;
     bool row_done = false;
