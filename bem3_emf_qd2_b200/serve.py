@@ -13,7 +13,7 @@ budget, evicting idle resident problems (least recently used first); requests th
 others are running are admitted as soon as memory and a worker free up, and run concurrently
 (each worker thread drives its contexts on its own CUDA stream).
 
-    python -m bem3_emf_qd2_b200.serve [--requests 48] [--workers 4] [--budget-gb 120] ...
+    python -m bem3_emf_qd2_b200.serve [--requests 48] [--workers 8] [--budget-gb 120] ...
 
 prints one JSON line: served solves/s at saturation, p50/p99 latency under a Poisson stream at
 80 % of that capacity, and the same requests solved one at a time by the plain drop-in path
@@ -344,7 +344,7 @@ def main():
     import tempfile
     ap = argparse.ArgumentParser()
     ap.add_argument("--requests", type=int, default=48)
-    ap.add_argument("--workers", type=int, default=4)
+    ap.add_argument("--workers", type=int, default=8)
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--load", type=float, default=0.8, help="Poisson rate as a fraction of the measured capacity")
     ap.add_argument("--no-sequential", action="store_true")
