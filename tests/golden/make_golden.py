@@ -18,11 +18,14 @@ from its sources by oracle/Makefile and called through oracle/reforacle.py:
                 results.
   potentials.npz  the reference's mEMP_s/_t/_i (types 0-3), EH_i and EH_mEMP_s/_t/_i (types
                 0-2) at the probe points and the near-boundary points of those results.
+  fullsize_rows.npz  rows of create_cmatrix_domain at the full sizes of the three plain
+                configurations (sphere384, twolayer3072, cone3360): dF, and G, H at every 8th column
+                and the element's own columns.
   power.npz     incident, reflected and transmitted power through one unit cell for those
                 results, from the reference's EH_t / EH_s on two planes.
 
 Usage: python tests/golden/make_golden.py [reference_dir] [section ...]
-       sections: gauleg faddeeva qpgf rows bv near potentials power (default: all)
+       sections: gauleg faddeeva qpgf rows bv near potentials power fullsize (default: all)
 """
 import os
 import sys
@@ -39,7 +42,7 @@ from bem3_emf_qd2_b200.dqd2 import load_inputs  # noqa: E402
 
 REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 SECTIONS = {a for a in sys.argv[2:] if "=" not in a} or {"gauleg", "faddeeva", "qpgf", "rows", "bv", "near",
-                                                         "potentials", "power"}
+                                                         "potentials", "power", "fullsize"}
 ONLY = {x for a in sys.argv[2:] if a.startswith("only=") for x in a[5:].split(",")}
 
 
@@ -199,8 +202,47 @@ def power_balance(o):
     np.savez_compressed(os.path.join(HERE, "power.npz"), **out)
 
 
+# elements whose rows the full-size fixture holds (1-based positions in each domain's list): the
+# rows where the double-layer identity F = 1/2 is least exact, and the first element
+FULLSIZE = {"sphere384": (1, 313), "twolayer3072": (1, 1536), "cone3360": (1, 69)}
+FULLSIZE_STRIDE = 8  # columns kept of each G, H row (every 8th, plus the self block)
+
+
+def fullsize_rows(o):
+    """Rows of create_cmatrix_domain at the three plain configurations' full sizes (meshes written
+    by bem3_emf_qd2_b200.meshgen and read by the reference's own readers): dF in full, G and H at
+    every FULLSIZE_STRIDE-th column and at the element's own four columns."""
+    import tempfile
+    from bem3_emf_qd2_b200 import meshgen
+    out = {}
+    for name, elems in FULLSIZE.items():
+        d = tempfile.mkdtemp(prefix="bem3_full_")
+        files = meshgen.make_config(name, d)
+        cwd = os.getcwd()
+        os.chdir(d)  # the reference keeps input file names in 64-byte buffers
+        try:
+            o.load(*[os.path.basename(f) for f in files])
+        finally:
+            os.chdir(cwd)
+        info = o.info()
+        for did in range(info["MN"] + 1):
+            for t in elems:
+                G, H, dG, dH, dF = o.assemble_rows(did, t, t)
+                N = G.shape[1]
+                cols = np.union1d(np.arange(0, N, FULLSIZE_STRIDE), np.arange(4 * (t - 1), 4 * t))
+                key = f"{name}/d{did}/t{t}"
+                out[key + "/cols"] = cols.astype(np.int32)
+                out[key + "/G"] = G[:, cols]
+                out[key + "/H"] = H[:, cols]
+                out[key + "/dF"] = dF
+                print(name, did, t, "done", flush=True)
+    np.savez_compressed(os.path.join(HERE, "fullsize_rows.npz"), **out)
+
+
 def main():
     o = RefOracle()
+    if "fullsize" in SECTIONS:
+        fullsize_rows(o)
     if "power" in SECTIONS:
         power_balance(o)
     if "near" in SECTIONS:
