@@ -512,14 +512,27 @@ static int ensure_tables(void)
 
 extern "C" void bem3_gauss_legendre(int n, double* x, double* w) { gauleg_host(n, x, w); }
 
-// Scratch needed for a chunk of `rows` rows: Fp (rows*ne double3) + GH list (rows*ne/8 + 4096 u32)
-size_t bem3_scratch_bytes(int ne, int rows)
+// Scratch layout of bem3_assemble_run for a chunk of `rows` rows, each part starting on a 256-byte
+// boundary: self-pair F sums (4 ne double3), the work-list counters (256 B), the chunk's per-pair F
+// terms (rows * ne double3), the near-singular work list (rows * ne / 8 + 4096 u32).
+static inline size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+struct ScratchLayout {
+  size_t fself, counters, fp, gh_list, end;
+  unsigned gh_cap;
+};
+static ScratchLayout scratch_layout(int ne, int rows)
 {
-  size_t np = (size_t)rows * ne;
-  size_t fp = np * sizeof(double3);
-  size_t gh = (np / 8 + 4096) * sizeof(unsigned);
-  return fp + gh + 256 + (size_t)4 * ne * sizeof(double3) + 256;
+  ScratchLayout l;
+  const size_t np = (size_t)rows * ne;
+  l.gh_cap = (unsigned)(np / 8 + 4096);
+  l.fself = 0;
+  l.counters = round256((size_t)4 * ne * sizeof(double3));
+  l.fp = l.counters + 256;
+  l.gh_list = l.fp + round256(np * sizeof(double3));
+  l.end = l.gh_list + round256((size_t)l.gh_cap * sizeof(unsigned));
+  return l;
 }
+size_t bem3_scratch_bytes(int ne, int rows) { return scratch_layout(ne, rows).end; }
 
 // Runs the whole domain on `stream` using caller-provided scratch (see bem3_scratch_bytes).
 // Returns 0, or a negative code (see bem3_qd2_b200.h).
@@ -536,17 +549,15 @@ int bem3_assemble_run(const AssembleArgs& A, const QPLattice* L, void* scratch, 
   const int ne = A.ne;
   const int nrows = 4 * ne;
   if (rows_per_chunk <= 0 || rows_per_chunk > nrows) rows_per_chunk = nrows;
-  if (bem3_scratch_bytes(ne, rows_per_chunk) > scratch_bytes) return BEM3_ERR_SCRATCH;
+  const ScratchLayout lay = scratch_layout(ne, rows_per_chunk);
+  if (lay.end > scratch_bytes) return BEM3_ERR_SCRATCH;  // every part below ends inside the scratch
   char* base = (char*)scratch;
-  double3* Fself = (double3*)base;
-  size_t off = ((size_t)nrows * sizeof(double3) + 255) & ~(size_t)255;
-  unsigned* gh_count = (unsigned*)(base + off);               // this chunk's list length
-  unsigned long long* gh_total = (unsigned long long*)(base + off + 8);  // the domain's total
-  off += 256;
-  double3* Fp = (double3*)(base + off);
-  off += (((size_t)rows_per_chunk * ne * sizeof(double3)) + 255) & ~(size_t)255;
-  unsigned* gh_list = (unsigned*)(base + off);
-  unsigned gh_cap = (unsigned)((size_t)rows_per_chunk * ne / 8 + 4096);
+  double3* Fself = (double3*)(base + lay.fself);
+  unsigned* gh_count = (unsigned*)(base + lay.counters);                          // this chunk's list length
+  unsigned long long* gh_total = (unsigned long long*)(base + lay.counters + 8);  // the domain's total
+  double3* Fp = (double3*)(base + lay.fp);
+  unsigned* gh_list = (unsigned*)(base + lay.gh_list);
+  const unsigned gh_cap = lay.gh_cap;
 
   const size_t N = (size_t)nrows;
   if (cudaMemsetAsync(A.G, 0, N * N * 16, st) != cudaSuccess) return BEM3_ERR_CUDA;

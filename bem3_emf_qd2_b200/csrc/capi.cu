@@ -452,7 +452,14 @@ extern "C" int bem3_assemble_domain_dev_noalloc(const double* geo_dev, int Ne, c
   int e = bem3_assemble_run(A, &L, scratch, avail, rows, status, st, &S);
   if (e) return e;
   int hs = 0;
+  unsigned long long gh = 0;
   if (cudaMemcpyAsync(&hs, status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return BEM3_ERR_CUDA;
+  if (cudaMemcpyAsync(&gh, S.d_gh_total, sizeof gh, cudaMemcpyDeviceToHost, st) != cudaSuccess) return BEM3_ERR_CUDA;
   if (cudaStreamSynchronize(st) != cudaSuccess) return BEM3_ERR_CUDA;
+  // this thread's counters, as the allocating entry fills them (no term counter or kernel timing:
+  // bem3_set_profiling does not apply to this entry point)
+  memset(&t_last_stats, 0, sizeof t_last_stats);
+  t_last_stats.gh_pairs = gh;
+  t_last_stats.launches = S.launches;
   return hs;
 }

@@ -97,7 +97,10 @@ int bem3_assemble_domain_dev(const double *geo_dev, int Ne, const int *sid_dev, 
  * domain) is rejected with BEM3_ERR_SCRATCH.  All calls share the array: calls that overlap on the
  * GPU (other streams, other threads on the same device) race and must be serialised by the caller.
  * The first call on a device resolves the array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  Synchronous on `stream`. */
+ * first call before any stream capture.  The address is kept for the life of the process, so the
+ * library must not be used on a device after cudaDeviceReset.  Synchronous on `stream`.  Fills
+ * bem3_last_gh_pairs and the gh_pairs / launches of bem3_last_stats; bem3_set_profiling (term
+ * counter, kernel timing) does not apply to it. */
 int bem3_assemble_domain_dev_noalloc(const double *geo_dev, int Ne, const int *sid_dev, int Ne_d, int did, int periodic,
                                      const bem3_qpd2 *qd, double kre, double kim, double *G_dev, double *H_dev,
                                      double *dG_dev, double *dH_dev, double *dF_dev, void *stream);

@@ -28,12 +28,15 @@ _cp = np.ctypeslib.ndpointer(dtype=np.complex128, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 
 
-def build(ref_dir: str = "/root/reference", quiet: bool = True) -> None:
-    """Build the oracle libraries (the reference part only when its sources exist)."""
+def build(ref_dir, quiet: bool = True) -> None:
+    """Build the oracle libraries.  ref_dir: a checkout of the reference, or None; the reference
+    part is built only when its sources are there, the C restatement always."""
     targets = ["port"]
-    if os.path.isdir(os.path.join(ref_dir, "d3qd2_src")):
+    args = []
+    if ref_dir and os.path.isdir(os.path.join(ref_dir, "d3qd2_src")):
         targets.insert(0, "ref")
-    out = subprocess.run(["make", "-C", HERE, f"REF={ref_dir}", "-j8", *targets],
+        args.append(f"REF={ref_dir}")
+    out = subprocess.run(["make", "-C", HERE, *args, "-j8", *targets],
                          capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout[-4000:] + out.stderr[-4000:])

@@ -1,8 +1,8 @@
 """Generates the golden fixtures in this directory from the reference (akohta/bem3_emf_qd2).
 
-Run in a checkout where the reference sources are present (default /root/reference) after
-``make -C oracle ref``.  Every array stored here comes from the reference's own code, compiled
-from its sources by oracle/Makefile and called through oracle/reforacle.py:
+Run with the path of a checkout of the reference's sources, after ``make -C oracle ref REF=<it>``.
+Every array stored here comes from the reference's own code, compiled from its sources by
+oracle/Makefile and called through oracle/reforacle.py:
 
   gauleg.npz    the Gauss-Legendre tables of gauleg (com_src/gauleg.c) for n = 12, 64
   faddeeva.npz  Faddeeva_w (qgf2_src/Faddeeva.cc) at seeded points, relerr 1e-15
@@ -23,9 +23,11 @@ from its sources by oracle/Makefile and called through oracle/reforacle.py:
                 and the element's own columns.
   power.npz     incident, reflected and transmitted power through one unit cell for those
                 results, from the reference's EH_t / EH_s on two planes.
+  c1_sphere384.npz  plain configuration 1 end to end through the reference's own solver program
+                (see c1_fixture).
 
-Usage: python tests/golden/make_golden.py [reference_dir] [section ...]
-       sections: gauleg faddeeva qpgf rows bv near potentials power fullsize (default: all)
+Usage: python tests/golden/make_golden.py <reference_dir> [section ...]
+       sections: gauleg faddeeva qpgf rows bv near potentials power fullsize c1 (default: all)
 """
 import os
 import sys
@@ -40,9 +42,11 @@ sys.path.insert(0, REPO)
 from reforacle import RefOracle  # noqa: E402
 from bem3_emf_qd2_b200.dqd2 import load_inputs  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2 or not os.path.isdir(os.path.join(sys.argv[1], "d3qd2_src")):
+    sys.exit("usage: make_golden.py <checkout of akohta/bem3_emf_qd2> [section ...]")
+REF = sys.argv[1]
 SECTIONS = {a for a in sys.argv[2:] if "=" not in a} or {"gauleg", "faddeeva", "qpgf", "rows", "bv", "near",
-                                                         "potentials", "power", "fullsize"}
+                                                         "potentials", "power", "fullsize", "c1"}
 ONLY = {x for a in sys.argv[2:] if a.startswith("only=") for x in a[5:].split(",")}
 
 
@@ -239,8 +243,84 @@ def fullsize_rows(o):
     np.savez_compressed(os.path.join(HERE, "fullsize_rows.npz"), **out)
 
 
+# Plain configuration 1 end to end (sphere384): elements whose complete rows are stored (1-based
+# positions in each domain's list, spread over the six cube faces), and the subset whose tangential
+# derivative rows dG, dH are stored too (interior domain; the open domain's are zero).
+C1_ROWS = [1 + 24 * i for i in range(16)]
+C1_DROWS = C1_ROWS[::2]
+C1_GRID = np.linspace(-0.5, 0.5, 21)  # probe grid on y = 0: x, z in [-0.5, 0.5] x period
+
+
+def c1_fixture(o):
+    """Plain configuration 1 (sphere384: cube-sphere r = 0.3 um of 384 quads, n = 1.59, square
+    lattice 1.0 um in n = 1.33, lambda0 = 0.6328, theta = 1e-4 rad) through the reference's own
+    programs: d3qd2_bv_solver (oracle/_ref, PARDISO replaced by a dense LU) writes the result
+    file, example1.out prints its probe field and force, and the reference's EH_t, force_FN and
+    create_cmatrix_domain give the rest.  Stored in c1_sphere384.npz:
+      in/*        the problem's inputs as the reference-format readers return them
+      bv{d}/*     boundary values of every domain (the result file's U, dU, E, H, dE, dH)
+      grid/*      EH_t, types 0 and 1, on the 21 x 21 probe grid of the y = 0 plane
+      force/*     force_FN types 0 and 1 about the origin
+      power/*     incident, reflected and transmitted power through one cell (plane_power)
+      rows/d{d}/t{t}/*  complete rows (G, H, dF; dG, dH for C1_DROWS of the interior domain)
+      example1    the stdout of the reference's example1.out on the result file
+    The solver run takes about half an hour on 8 cores; BEM3_C1_WORKDIR may name a directory that
+    holds a finished run (c1.dat) to reuse."""
+    import subprocess
+    import tempfile
+    from bem3_emf_qd2_b200 import meshgen, plane_power
+    d = os.environ.get("BEM3_C1_WORKDIR") or tempfile.mkdtemp(prefix="bem3_c1_")
+    files = meshgen.make_config("sphere384", d)
+    names = [os.path.basename(f) for f in files]
+    ref_bin = os.path.join(REPO, "oracle", "_ref")
+    if not os.path.exists(os.path.join(d, "c1.dat")):
+        with open(os.path.join(d, "solver.log"), "w") as log:
+            subprocess.run([os.path.join(ref_bin, "d3qd2_bv_solver"), *names, "c1.dat"], cwd=d, check=True,
+                           stdout=log, stderr=subprocess.STDOUT)
+    ex1 = subprocess.run([os.path.join(ref_bin, "example1.out"), "c1.dat"], cwd=d, check=True,
+                         capture_output=True, text=True).stdout
+    rec = {"in/" + k: v for k, v in load_inputs(*files).items()}
+    rec["example1"] = np.array(ex1)
+    cwd = os.getcwd()
+    os.chdir(d)  # the reference keeps file names in 64-byte buffers
+    try:
+        o.load_dat("c1.dat")
+    finally:
+        os.chdir(cwd)
+    info = o.info()
+    for dd in range(info["MN"] + 1):
+        for k, v in o.boundary_values(dd).items():
+            rec[f"bv{dd}/{k}"] = v
+    X, Z = np.meshgrid(C1_GRID, C1_GRID, indexing="ij")
+    r = np.c_[X.ravel(), np.zeros(X.size), Z.ravel()]
+    rec["grid/r"] = r
+    for ty in (0, 1):
+        E, H, did = o.EH(r, ty, total=True)
+        rec[f"grid/E{ty}"], rec[f"grid/H{ty}"], rec["grid/did"] = E, H, did
+        F, N = o.force((0.0, 0.0, 0.0), ty)
+        rec[f"force/F{ty}"], rec[f"force/N{ty}"] = F, N
+    print("c1 grid and force done", flush=True)
+    from bem3_emf_qd2_b200.dqd2 import problem_from_arrays
+    p = problem_from_arrays({k[3:]: v for k, v in rec.items() if k.startswith("in/")})
+    pw = plane_power(lambda x, total: o.EH(x, 0, total=total), p.vd1, p.vd2, p.waves[0].cos_t > 0, 0.6, -0.6, 16)
+    for k, v in pw.items():
+        rec[f"power/{k}"] = np.array(v)
+    print("c1 power", pw, flush=True)
+    for dd in range(info["MN"] + 1):
+        for t in C1_ROWS:
+            G, H, dG, dH, dF = o.assemble_rows(dd, t, t)
+            key = f"rows/d{dd}/t{t}"
+            rec[key + "/G"], rec[key + "/H"], rec[key + "/dF"] = G, H, dF
+            if dd > 0 and t in C1_DROWS:
+                rec[key + "/dG"], rec[key + "/dH"] = dG, dH
+        print("c1 rows of domain", dd, "done", flush=True)
+    np.savez_compressed(os.path.join(HERE, "c1_sphere384.npz"), **rec)
+
+
 def main():
     o = RefOracle()
+    if "c1" in SECTIONS:
+        c1_fixture(o)
     if "fullsize" in SECTIONS:
         fullsize_rows(o)
     if "power" in SECTIONS:

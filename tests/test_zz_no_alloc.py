@@ -61,12 +61,15 @@ def _check(B, P, did):
     ref = _outputs(torch, ne, dev)
     assert _run(B.lib().bem3_assemble_domain_dev, B, P, dp, did, ref) == 0
     torch.cuda.synchronize()
+    gh_ref = B.lib().bem3_last_gh_pairs()
     fn = _entry(B)
     for call in range(2):
         got = _outputs(torch, ne, dev)
         rc = _run(fn, B, P, dp, did, got)
         assert rc == 0, (did, call, rc)
         torch.cuda.synchronize()
+        # the counters of this thread's last assembly come from this call, not an earlier one
+        assert B.lib().bem3_last_gh_pairs() == gh_ref, (did, call)
         for name in ("G", "H", "dG", "dH", "dF"):
             r, g = ref[name], got[name]
             assert bool(torch.isfinite(r).all()), name
