@@ -100,9 +100,11 @@ def lib():
     """The loaded CUDA library (raises if it is not built)."""
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise RuntimeError(f"CUDA library not built: {LIB_PATH} (run bem3_emf_qd2_b200.build())")
-        L = C.CDLL(LIB_PATH)
+        # BEM3_QD2_LIB: another build of the same library (e.g. a variant compiled with other -D options)
+        path = os.environ.get("BEM3_QD2_LIB", LIB_PATH)
+        if not os.path.exists(path):
+            raise RuntimeError(f"CUDA library not built: {path} (run bem3_emf_qd2_b200.build())")
+        L = C.CDLL(path)
         vp, i, d = C.c_void_p, C.c_int, C.c_double
         L.bem3_qpgf.argtypes = [C.POINTER(bem3_qpd2), i, vp, vp, vp, i]
         L.bem3_qpgf_dev.argtypes = [C.POINTER(bem3_qpd2), i, vp, vp, vp, i, vp]
@@ -118,6 +120,7 @@ def lib():
         L.bem3_ctx_set_solver.argtypes = [vp, i]
         L.bem3_ctx_set_incident.argtypes = [vp, i, vp, vp, vp, vp, vp]
         L.bem3_ctx_resolve.argtypes = [vp]
+        L.bem3_ctx_phase_times.argtypes = [vp, vp]
         L.bem3_ctx_release.argtypes = [vp]
         L.bem3_ctx_device_bytes.argtypes = [vp]
         L.bem3_ctx_device_bytes.restype = C.c_size_t
@@ -343,6 +346,13 @@ class Context:
         """method 0: reduced 4 NN system where applicable, 1: the full 8 NN system, 2: reduced only."""
         check(lib().bem3_ctx_set_solver(self.h, method), "bem3_ctx_set_solver")
         check(lib().bem3_ctx_solve(self.h), "bem3_ctx_solve")
+
+    def phase_times(self) -> dict:
+        """Device time (ms) of the last solve's phases -- bem3_ctx_phase_times: the coefficient
+        matrices, the factorisations, the right-hand sides with the boundary fields."""
+        ms = (C.c_double * 3)()
+        check(lib().bem3_ctx_phase_times(self.h, ms), "bem3_ctx_phase_times")
+        return dict(assembly_ms=ms[0], factor_ms=ms[1], rhs_fields_ms=ms[2])
 
     def set_incident(self, waves) -> None:
         """Replace the incident plane waves (same wavelength and direction as the solved ones; the

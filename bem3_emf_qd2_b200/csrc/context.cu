@@ -37,6 +37,7 @@ struct bem3_ctx_s {
   DevBuf status;
   DevBuf prop;  // the lattice's propagating orders (the optimised lattice sums of the self rule)
   SolveState* st = nullptr;
+  double phase_ms[3] = {0.0, 0.0, 0.0};  // last solve: assembly, factorisation, right-hand sides + fields
   ~bem3_ctx_s() { delete st; }
 };
 
@@ -562,6 +563,34 @@ extern "C" int bem3_ctx_set_solver(bem3_ctx c, int method)
   return 0;
 }
 
+namespace {
+// CUDA events around the solve's phases on the calling thread's stream (the one all its work goes to).
+struct PhaseClock {
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool ok = true;
+  PhaseClock()
+  {
+    for (auto& e : ev)
+      if (cudaEventCreate(&e) != cudaSuccess) { e = nullptr; ok = false; }
+  }
+  ~PhaseClock()
+  {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+  void mark(int i) { if (ok) cudaEventRecord(ev[i], cudaStreamPerThread); }
+  // elapsed ms between marks lo..hi into out[], after waiting for the last mark
+  void read(int lo, int hi, double* out)
+  {
+    if (!ok || cudaEventSynchronize(ev[hi]) != cudaSuccess) return;
+    for (int i = lo; i < hi; i++) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev[i], ev[i + 1]) == cudaSuccess) out[i - lo] = ms;
+    }
+  }
+};
+}  // namespace
+
 extern "C" int bem3_ctx_solve(bem3_ctx c)
 {
   if (!c) return BEM3_ERR_ARG;
@@ -569,15 +598,34 @@ extern "C" int bem3_ctx_solve(bem3_ctx c)
   delete c->st;
   c->st = new SolveState();
   SolveState& T = *c->st;
+  PhaseClock clk;
+  clk.mark(0);
   int rc = phase_assemble(c, T);
   if (rc) { delete c->st; c->st = nullptr; return rc; }
+  clk.mark(1);
   SolveDev S = solve_view_with(c, T);
   Handles& hd = thread_handles(c->dev);
-  if ((rc = hd.init()) || (rc = phase_factor(c, T, S, hd)) || (rc = phase_rhs(c, T, S, hd))) {
+  if ((rc = hd.init()) || (rc = phase_factor(c, T, S, hd))) {
     delete c->st;
     c->st = nullptr;
     return rc;
   }
+  clk.mark(2);
+  if ((rc = phase_rhs(c, T, S, hd))) {
+    delete c->st;
+    c->st = nullptr;
+    return rc;
+  }
+  clk.mark(3);
+  c->phase_ms[0] = c->phase_ms[1] = c->phase_ms[2] = 0.0;
+  clk.read(0, 3, c->phase_ms);
+  return 0;
+}
+
+extern "C" int bem3_ctx_phase_times(bem3_ctx c, double* ms)
+{
+  if (!c || !ms) return BEM3_ERR_ARG;
+  for (int i = 0; i < 3; i++) ms[i] = c->phase_ms[i];
   return 0;
 }
 
@@ -611,7 +659,14 @@ extern "C" int bem3_ctx_resolve(bem3_ctx c)
   SolveDev S = solve_view_with(c, T);
   Handles& hd = thread_handles(c->dev);
   int rc = hd.init();
+  PhaseClock clk;
+  clk.mark(2);
   if (!rc) rc = phase_rhs(c, T, S, hd);
+  clk.mark(3);
+  if (!rc) {
+    c->phase_ms[0] = c->phase_ms[1] = c->phase_ms[2] = 0.0;
+    clk.read(2, 3, c->phase_ms + 2);
+  }
   return rc;
 }
 

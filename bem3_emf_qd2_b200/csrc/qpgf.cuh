@@ -37,6 +37,14 @@
 #define QP_EFS 0.1
 #define QP_MEPS 1.0e-15
 #define QP_PROP_CAP 2048  // most propagating orders a hoisted lattice list holds
+#ifndef QP_EW_REC
+#define QP_EW_REC 1  // Gaussian recurrence for the Ewald spectral rows' exponential (assembly form)
+#endif
+#ifndef QP_FD_ZFAC
+// Fourier-domain sum in the assembly's evaluation (OPT) only for |z| > QP_FD_ZFAC x split parameter:
+// (39 / 6.1) sqrt(c), c = cost of a Fourier evanescent term / cost of an Ewald one (measured on B200)
+#define QP_FD_ZFAC 4.5
+#endif
 #define QP_PI 3.14159265358979323846
 #define QP_INV_SQRTPI 5.6418958354775628695e-1
 
@@ -236,6 +244,27 @@ BEM_HD void qp_ew2_evan(const double* r, double veps, double an0, double an1, do
   dF[1] = F * an1;
   dF[2] = ce * (f1 - f2);
 }
+// The FAST form with its exponential E = e^{-a^2 - b^2} = e^{(k^2 - |a_n|^2) veps^2 - z^2 / (4 veps^2)}
+// supplied by the caller, which carries it along a row of the spectral sum by a recurrence.
+BEM_HD void qp_ew2_evan_E(const double* r, double veps, double an0, double an1, double bn, double ibn, double E,
+                          cplx ce, cplx& F, cplx* dF)
+{
+  BEM_STAT_T(2);
+  const double azve = r[2] / (2.0 * veps);
+  const double a = bn * veps;
+  double x1 = 0.0, x2 = 0.0;
+#pragma unroll 1
+  for (int j = 0; j < 2; j++) {
+    const double v = qp_erfcx(j == 0 ? a + azve : fabs(a - azve));
+    if (j == 0) x1 = v; else x2 = v;
+  }
+  const double f1 = E * x1;
+  const double f2 = (a >= azve) ? E * x2 : 2.0 * qp_exp(-bn * r[2]) - E * x2;
+  F = mul_mi(ce * ((f1 + f2) * ibn));
+  dF[0] = F * an0;
+  dF[1] = F * an1;
+  dF[2] = ce * (f1 - f2);
+}
 // Returns 0 propagating, 1 evanescent, -3 when beta_n == 0 exactly.
 template <bool FAST = false>
 BEM_HD int qp_ew2_term(const QPLattice& L, const double* r, double veps, int n1, int n2, cplx ce, cplx& F, cplx* dF)
@@ -415,6 +444,15 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
   const int nc = L.nc1;
   const cplx E2 = expi(L.g2x * r[0] + L.g2y * r[1]);  // phase step along n2
   int dir = 0, n1 = nc, side = -1, off = 0, flg = 0;
+  // OPT Ewald rows: the factor E(n2) = e^{(k^2 - |a_n|^2) veps^2 - z^2 / (4 veps^2)} of the evanescent
+  // terms by a Gaussian recurrence along the row.  |a_n|^2 is quadratic in n2 (a_n = c + n2 g2), so
+  // E(n2 +- 1) = E(n2) R, with the ratio R itself multiplied by Cg = e^{-2 |g2|^2 veps^2} per step:
+  // two multiplications per term instead of an exponential.  Exact in exact arithmetic; each step adds
+  // about one rounding, which stays far below the terms' 1e-16 stop threshold over the row lengths here.
+  const bool rec = QP_EW_REC && OPT && !FD;
+  const double ve2 = veps * veps, azv = r[2] / (2.0 * veps);
+  const double Cg = rec ? qp_exp(-2.0 * L.g22 * ve2) : 0.0;
+  double Ec0 = 0.0, Rp0 = 0.0, Rm0 = 0.0, Ecur = 0.0, Rcur = 0.0;
   int nc2;
   if (FD) nc2 = (int)round((L.vkx * L.g2x + L.vky * L.g2y - (double)n1 * L.g12) / L.g22);
   else nc2 = (int)round(-((-L.vkx + (double)n1 * L.g1x) * L.g2x + (-L.vky + (double)n1 * L.g1y) * L.g2y) / L.g22);
@@ -429,6 +467,13 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
       const double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
       const double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
       const double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
+      if (rec && side < 0) {  // row centre: the recurrence's start and its first ratio on each side
+        const double adg = an0 * L.g2x + an1 * L.g2y;
+        Ec0 = qp_exp(bn2 * ve2 - azv * azv);
+        Rp0 = qp_exp(-(2.0 * adg + L.g22) * ve2);
+        Rm0 = qp_exp((2.0 * adg - L.g22) * ve2);
+        Ecur = Ec0;
+      }
       if (bn2 > 0.0) {
         e = 2;
       } else if (bn2 < 0.0) {
@@ -436,6 +481,7 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
         const double ibn = rsqrt_(-bn2);
         const double bn = -bn2 * ibn;
         if (FD) qp_fd_evan(r, an0, an1, bn, ibn, ph, F, dF);
+        else if (rec) qp_ew2_evan_E(r, veps, an0, an1, bn, ibn, Ecur, ph, F, dF);
         else qp_ew2_evan<OPT>(r, veps, an0, an1, bn, ibn, ph, F, dF);
         e = 1;
       } else {
@@ -452,6 +498,7 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
     }
     if (side < 0) {
       side = 0; off = 1; ph = ph0 * E2;
+      if (rec) { Ecur = Ec0 * Rp0; Rcur = Rp0 * Cg; }
       continue;
     }
     bool stop = false;
@@ -465,10 +512,12 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
       if (off + 1 >= LIMIT) return ELIM;
       off++;
       ph = ph * (side == 0 ? E2 : conj(E2));
+      if (rec) { Ecur *= Rcur; Rcur *= Cg; }
       continue;
     }
     if (side == 0) {
       side = 1; off = 1; ph = ph0 * conj(E2);
+      if (rec) { Ecur = Ec0 * Rm0; Rcur = Rm0 * Cg; }
       continue;
     }
     // row finished
@@ -554,16 +603,24 @@ QP_EVAL_FN int qpgf_eval(const QPLattice& L, const double* r_in, QPVal& out)
   if (!L.ew_only) {
     use_fd = (L.bN / L.bNp * exp(-L.bNp * fabs(r[2])) < eps) && (L.bN / L.bNm * exp(-L.bNm * fabs(r[2])) < eps);
   }
+  // split parameter (d3_qpgf_d2.c:1683-1693)
+  double veps = L.veps0;
+  {
+    const double r2_min = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    if (L.k * L.k * veps * veps - r2_min / (4.0 * veps * veps) > QP_EW_EXPM)
+      veps = sqrt(QP_EW_EXPM + sqrt(L.k * L.k * r2_min + QP_EW_EXPM * QP_EW_EXPM)) / (sqrt(2.0) * L.k);
+  }
+  // OPT: the Fourier-domain sum only where it is also the cheaper one.  Its evanescent orders decay
+  // as e^{-beta |z|}, so it needs the orders with |beta| up to ~39 / |z| (a 1e-17 decay); the Ewald
+  // sums need those with |beta| up to ~6.1 / veps (erfc below 1e-17) plus a few real-space terms.
+  // Both converge to the same value (to ~1e-13 relative on the assembly's points), so the choice is
+  // by cost: Fourier only when |z| > QP_FD_ZFAC veps.
+  if (OPT && use_fd && fabs(r[2]) < QP_FD_ZFAC * veps) use_fd = false;
   int err;
   if (use_fd) {
     err = qp_spec_sum<MODE, 1, OPT>(L, r, 0.0, eps, out.G, out.dG);
     if (err < 0) return err - 10;
   } else {
-    // split parameter (d3_qpgf_d2.c:1683-1693)
-    double veps = L.veps0;
-    double r2_min = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-    if (L.k * L.k * veps * veps - r2_min / (4.0 * veps * veps) > QP_EW_EXPM)
-      veps = sqrt(QP_EW_EXPM + sqrt(L.k * L.k * r2_min + QP_EW_EXPM * QP_EW_EXPM)) / (sqrt(2.0) * L.k);
     cplx S2, dS2[3];
     int c1 = qp_ew1_sum<MODE, OPT>(L, r, veps, eps, out.G, out.dG);
     if (c1 < 0) return c1 - 20;

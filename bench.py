@@ -31,15 +31,19 @@ sys.path.insert(0, REPO)
 
 METRIC = "QPGF element-pair evals/s"
 UNIT = "pairs/s"
-# FP64 operations per lattice-sum term of the regular periodic kernel, per workload: the
-# FP64 instructions ncu counts in one launch (2 DFMA + DADD + DMUL, thread level) divided by the
-# terms the kernel's own counter reports for that launch, captured on the workload's /stride8
-# subsample (same lattice, wavelength and element size).  The live roofline figure is
-# terms/s x this number.
-FP64_OPS_PER_TERM = {"twolayer3072": 198.6}
+# Algorithmic FP64 operations per lattice-sum term of the regular periodic pairs, per workload:
+# oracle/opcount.py (the CPU restatement of the lattice sums on an operation-counting number type,
+# special functions at the counts of compact published methods, per-point element work included)
+# over a seeded sample of 96 of the workload's regular periodic pairs, with the assembly's method
+# choice.  Fixed: the kernel's own instruction count is reported beside it, not in its place.
+ALG_OPS_PER_TERM = {"twolayer3072": 378.23, "sphere384": 377.03, "cone3360": 398.91}
+# FP64 operations per term the hardware executed in k_reg_periodic (ncu: 2 x DFMA + DADD + DMUL,
+# thread level, over the kernel's own term counter), from the capture of the workload's /stride8
+# subsample in profiles/; None where no capture of the current kernel exists.
+HW_OPS_PER_TERM = {}
 # DRAM bytes (read + write) of one k_reg_periodic launch, from the same capture scaled by the
 # pairs processed (64x for stride 8).
-TRAFFIC_PER_LAUNCH = {"twolayer3072": 1.4194e9 * 64}
+TRAFFIC_PER_LAUNCH = {}
 
 
 def parse():
@@ -296,17 +300,17 @@ def run_ours(args):
     if reg_launches:
         per_launch_ms = reg_ms / reg_launches
         terms_per_launch = terms / reg_launches
-        ops = FP64_OPS_PER_TERM.get(args.config)
-        if ops:
-            achieved = terms_per_launch * ops / (per_launch_ms * 1e-3) / 1e12
-            roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": TRAFFIC_PER_LAUNCH.get(args.config),
-                    "fp64_ops_per_term": ops,
-                    "kernel": "k_reg_periodic", "peak_source": "measured DFMA probe on this GPU"}
-        else:
-            roof = {"bound": "fp64", "achieved": None, "peak": peak, "unit": "TFLOP/s", "frac": None,
-                    "traffic": None, "kernel": "k_reg_periodic",
-                    "terms_per_s": terms_per_launch / (per_launch_ms * 1e-3)}
+        ops = ALG_OPS_PER_TERM.get(args.config)
+        hw = HW_OPS_PER_TERM.get(args.config)
+        achieved = terms_per_launch * ops / (per_launch_ms * 1e-3) / 1e12 if ops else None
+        roof = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if achieved else None,
+                "traffic": TRAFFIC_PER_LAUNCH.get(args.config), "kernel": "k_reg_periodic",
+                "peak_source": "measured DFMA probe on this GPU (MEASURED_PEAKS.json has no FP64 entry)",
+                "alg_ops_per_term": ops, "ops_basis": "oracle/opcount.py: restatement op count, seeded sample",
+                "hw_ops_per_term": hw,
+                "hw_frac": terms_per_launch * hw / (per_launch_ms * 1e-3) / 1e12 / peak if hw else None,
+                "terms_per_s": terms_per_launch / (per_launch_ms * 1e-3)}
         roof["launch_ms"] = per_launch_ms
         roof["terms_per_launch"] = terms_per_launch
 

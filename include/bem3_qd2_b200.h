@@ -210,6 +210,14 @@ int bem3_ctx_set_solver(bem3_ctx c, int method);
  * (same layouts), bem3_ctx_resolve recomputes the boundary values.  bem3_ctx_release frees the
  * matrices and factorisations and keeps the boundary values.  No counterpart in the reference,
  * which assembles and factorises for every run. */
+/* Device time (ms, CUDA events) of the last bem3_ctx_solve's phases, the three that the reference's
+ * solve_bieq reports (d3qd2_solve_bieq.c:48-83): ms[0] the coefficient matrices of every domain
+ * (create_cmatrix), ms[1] the factorisations (every domain's compacted G and the system of the
+ * potentials: create_tmatrix_csr + solve_tmatrix_csr's factorisation), ms[2] the right-hand sides,
+ * the boundary values, E, H and dE, dH on the boundary (tmatrix_bd_store, q1_solve_eh_bv,
+ * solve_deh_bv).  After bem3_ctx_resolve, ms[0] = ms[1] = 0 and ms[2] is the re-solve. */
+int bem3_ctx_phase_times(bem3_ctx c, double *ms /* [3] */);
+
 int bem3_ctx_set_incident(bem3_ctx c, int nwaves, const bem3_wave *waves, const double *Ui, const double *dUi,
                           const double *dEiz, const double *dEie);
 int bem3_ctx_resolve(bem3_ctx c);
