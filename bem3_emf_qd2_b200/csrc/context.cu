@@ -834,6 +834,45 @@ extern "C" int bem3_ctx_force(bem3_ctx c, const double* rc, int type, double* F,
   return hs;
 }
 
+extern "C" int bem3_ctx_field_bd(bem3_ctx c, int did, int n, const int* t, const double* zeta_eta, int type,
+                                 int total, double* E, double* H)
+{
+  if (!c || n < 0 || (n > 0 && (!t || !zeta_eta || !E || !H)) || type < 0 || type > 3 || total < 0 || total > 1)
+    return BEM3_ERR_ARG;
+  // the open region of a quasi-periodic problem only: the element's own integral uses the periodic
+  // self rule (interior domains would need the free-space rule of coef_bd at arbitrary points)
+  if (did != 0 || c->ps != 1) return BEM3_ERR_ARG;
+  if (n == 0) return 0;
+  const int ne = (int)c->sid[0].size();
+  std::vector<int> tl((size_t)n);
+  for (int i = 0; i < n; i++) {
+    if (t[i] < 1 || t[i] > ne) return BEM3_ERR_ARG;
+    tl[(size_t)i] = t[i] - 1;
+  }
+  DeviceGuard g(c->dev);
+  if (ensure_tables() != 0) return BEM3_ERR_CUDA;
+  ForceArgs A;
+  memset(&A, 0, sizeof A);
+  A.geo = c->geo.as<double>(); A.ne = ne; A.sid = c->dsid[0].as<int>();
+  A.E = c->E[0].as<double>(); A.dE = c->dE[0].as<double>(); A.H = c->H[0].as<double>(); A.dH = c->dH[0].as<double>();
+  A.k0re = c->kn[0]; A.k0im = c->kn[1];
+  A.waves = c->waves.as<bem3_wave>(); A.nwaves = c->nwaves;
+  DevBuf dt, dze, dE, dH;
+  int rc;
+  if ((rc = upload(dt, tl.data(), (size_t)n)) || (rc = upload(dze, zeta_eta, (size_t)2 * n))) return rc;
+  if (dE.alloc((size_t)n * 6 * sizeof(double)) || dH.alloc((size_t)n * 6 * sizeof(double))) return BEM3_ERR_CUDA;
+  cudaMemset(c->status.p, 0, sizeof(int));
+  k_field_bd<<<(unsigned)n, FORCE_THREADS>>>(A, c->L, n, dt.as<int>(), dze.as<double>(), type, total, dE.as<double>(),
+                                             dH.as<double>(), c->status.as<int>());
+  if (cudaGetLastError() != cudaSuccess) return BEM3_ERR_CUDA;
+  int hs = 0;
+  if (cudaMemcpy(&hs, c->status.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(E, dE.p, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(H, dH.p, (size_t)n * 6 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return BEM3_ERR_CUDA;
+  return hs;
+}
+
 extern "C" int bem3_solve_bieq_arrays(const bem3_problem* P, bem3_bv* out)
 {
   if (!out) return BEM3_ERR_ARG;

@@ -86,6 +86,102 @@ __device__ __forceinline__ void fblock_sum(double (*red)[FORCE_THREADS], double*
   }
 }
 
+// Scattered field of the open region at the point r = r(z, e) of its element t (0-based position in the
+// domain's list, element id at): every other element's coefficients by the rule `type` (0-3, as
+// q0_coef_bd takes them for s != t, d3qd2_elem.c), the element itself by the singular rule around
+// (z, e) (the periodic self rule, self.cuh), combined with the boundary values and divided by 1 + F
+// (EH_s_bd, d3qd2_field.c:299-341).  Called by every thread of a FORCE_THREADS block; the result is
+// valid in thread 0.  red: the block's reduction buffer.
+__device__ void bd_field_block(const ForceArgs& A, const QPLattice& L, int t, int at, double z, double e,
+                               const double* r, int type, int* status, double (*red)[FORCE_THREADS], cplx* es,
+                               cplx* hs)
+{
+  const cplx k = mk(A.k0re, A.k0im);
+  cplx ea[3], ha[3];
+  for (int l = 0; l < 3; l++) { ea[l] = mk(0, 0); ha[l] = mk(0, 0); }
+  double F = 0.0;
+  for (int s = threadIdx.x; s < A.ne; s += FORCE_THREADS) {
+    if (s == t) continue;
+    cplx CC[8];
+    double f;
+    const int st = field_coef<true>(A.geo, A.sid[s], r, k, type, L, CC, f);
+    if (st < 0) record_status(status, st);
+    const size_t b = (size_t)(4 * (s + 1)) * 3;
+    for (int n = 0; n < 4; n++)
+      for (int l = 0; l < 3; l++) {
+        const size_t q = 2 * (b + 3 * n + l);
+        ea[l] += CC[n] * mk(A.dE[q], A.dE[q + 1]) - CC[n + 4] * mk(A.E[q], A.E[q + 1]);
+        ha[l] += CC[n] * mk(A.dH[q], A.dH[q + 1]) - CC[n + 4] * mk(A.H[q], A.H[q + 1]);
+      }
+    F += f;
+  }
+  SelfInfo S;
+  self_setup_at(A.geo, at, z, e, k, S);
+  double sv[24];
+  for (int j = 0; j < 24; j++) sv[j] = 0.0;
+  const int st = self_per_points(S, L, c_xl, c_wl, c_xh, c_wh, threadIdx.x, FORCE_THREADS, sv, 1);
+  if (st < 0) record_status(status, st);
+  double v[37];
+  for (int l = 0; l < 3; l++) {
+    v[2 * l] = ea[l].re; v[2 * l + 1] = ea[l].im; v[6 + 2 * l] = ha[l].re; v[7 + 2 * l] = ha[l].im;
+  }
+  v[12] = F;
+  for (int j = 0; j < 24; j++) v[13 + j] = sv[j];
+  fblock_sum<37>(red, v);
+  if (threadIdx.x == 0) {
+    double R[24];
+    for (int j = 0; j < 24; j++) R[j] = red[13 + j][0];
+    cplx CC[9], dCz[9], dCe[9];
+    self_per_combine(S, R, CC, dCz, dCe);
+    for (int l = 0; l < 3; l++) { es[l] = mk(red[2 * l][0], red[2 * l + 1][0]); hs[l] = mk(red[6 + 2 * l][0], red[7 + 2 * l][0]); }
+    const size_t b = (size_t)(4 * (t + 1)) * 3;
+    for (int n = 0; n < 4; n++)
+      for (int l = 0; l < 3; l++) {
+        const size_t q = 2 * (b + 3 * n + l);
+        es[l] += CC[n] * mk(A.dE[q], A.dE[q + 1]) - CC[n + 4] * mk(A.E[q], A.E[q + 1]);
+        hs[l] += CC[n] * mk(A.dH[q], A.dH[q + 1]) - CC[n + 4] * mk(A.H[q], A.H[q + 1]);
+      }
+    const double sc = 1.0 / (1.0 + red[12][0] + CC[8].re);
+    for (int l = 0; l < 3; l++) { es[l] = es[l] * sc; hs[l] = hs[l] * sc; }
+  }
+  __syncthreads();
+}
+
+// Field on the open region's boundary at n points (element position t[i], parameters ze[2 i], ze[2 i + 1]):
+// scattered (total 0, EH_s_bd) or plus the incident field (total 1, EH_t_bd, d3qd2_field.c:343-385).
+// One block per point; E, H: [n][3] complex.
+__global__ void __launch_bounds__(FORCE_THREADS) k_field_bd(ForceArgs A, const __grid_constant__ QPLattice L, int n,
+                                                            const int* __restrict__ tl, const double* __restrict__ ze,
+                                                            int type, int total, double* __restrict__ E,
+                                                            double* __restrict__ H, int* status)
+{
+  const int i = blockIdx.x;
+  if (i >= n) return;
+  const int t = tl[i];
+  const int at = abs(A.sid[t]);
+  const double z = ze[2 * i], e = ze[2 * i + 1];
+  Elem el;
+  load_elem(A.geo, at, el);
+  double r[3];
+  if (el.nn == 4) {
+    double w[3];
+    bil_rw(el, z, e, r, w);
+  } else {
+    lit_r(el, z, e, r);
+  }
+  __shared__ double red[37][FORCE_THREADS];
+  cplx es[3], hs[3];
+  bd_field_block(A, L, t, at, z, e, r, type, status, red, es, hs);
+  if (threadIdx.x != 0) return;
+  cplx ei[3], hi[3];
+  if (total) force_incident(A, r, ei, hi);
+  for (int l = 0; l < 3; l++) {
+    const cplx ev = total ? es[l] + ei[l] : es[l], hv = total ? hs[l] + hi[l] : hs[l];
+    E[6 * (size_t)i + 2 * l] = ev.re; E[6 * (size_t)i + 2 * l + 1] = ev.im;
+    H[6 * (size_t)i + 2 * l] = hv.re; H[6 * (size_t)i + 2 * l + 1] = hv.im;
+  }
+}
+
 __global__ void __launch_bounds__(FORCE_THREADS) k_force_points(ForceArgs A, const __grid_constant__ QPLattice L,
                                                                double* __restrict__ out, int* status)
 {
@@ -128,57 +224,13 @@ __global__ void __launch_bounds__(FORCE_THREADS) k_force_points(ForceArgs A, con
   } else {
     // boundary field at r (EH_t_bd): other elements by the nodal rule, the element itself by the
     // singular rule around (z, e)
-    const cplx k = mk(A.k0re, A.k0im);
-    cplx ea[3], ha[3];
-    for (int l = 0; l < 3; l++) { ea[l] = mk(0, 0); ha[l] = mk(0, 0); }
-    double F = 0.0;
-    for (int s = threadIdx.x; s < A.ne; s += FORCE_THREADS) {
-      if (s == t) continue;
-      cplx CC[8];
-      double f;
-      const int st = field_coef<true>(A.geo, A.sid[s], r, k, 0, L, CC, f);
-      if (st < 0) record_status(status, st);
-      const size_t b = (size_t)(4 * (s + 1)) * 3;
-      for (int n = 0; n < 4; n++)
-        for (int l = 0; l < 3; l++) {
-          const size_t q = 2 * (b + 3 * n + l);
-          ea[l] += CC[n] * mk(A.dE[q], A.dE[q + 1]) - CC[n + 4] * mk(A.E[q], A.E[q + 1]);
-          ha[l] += CC[n] * mk(A.dH[q], A.dH[q + 1]) - CC[n + 4] * mk(A.H[q], A.H[q + 1]);
-        }
-      F += f;
-    }
-    SelfInfo S;
-    self_setup_at(A.geo, at, z, e, k, S);
-    double sv[24];
-    for (int j = 0; j < 24; j++) sv[j] = 0.0;
-    const int st = self_per_points(S, L, c_xl, c_wl, c_xh, c_wh, threadIdx.x, FORCE_THREADS, sv, 1);
-    if (st < 0) record_status(status, st);
-    double v[37];
-    for (int l = 0; l < 3; l++) {
-      v[2 * l] = ea[l].re; v[2 * l + 1] = ea[l].im; v[6 + 2 * l] = ha[l].re; v[7 + 2 * l] = ha[l].im;
-    }
-    v[12] = F;
-    for (int j = 0; j < 24; j++) v[13 + j] = sv[j];
-    fblock_sum<37>(red, v);
+    cplx es[3], hs[3];
+    bd_field_block(A, L, t, at, z, e, r, 0, status, red, es, hs);
     if (threadIdx.x == 0) {
-      double R[24];
-      for (int j = 0; j < 24; j++) R[j] = red[13 + j][0];
-      cplx CC[9], dCz[9], dCe[9];
-      self_per_combine(S, R, CC, dCz, dCe);
-      cplx es[3], hs[3];
-      for (int l = 0; l < 3; l++) { es[l] = mk(red[2 * l][0], red[2 * l + 1][0]); hs[l] = mk(red[6 + 2 * l][0], red[7 + 2 * l][0]); }
-      const size_t b = (size_t)(4 * (t + 1)) * 3;
-      for (int n = 0; n < 4; n++)
-        for (int l = 0; l < 3; l++) {
-          const size_t q = 2 * (b + 3 * n + l);
-          es[l] += CC[n] * mk(A.dE[q], A.dE[q + 1]) - CC[n + 4] * mk(A.E[q], A.E[q + 1]);
-          hs[l] += CC[n] * mk(A.dH[q], A.dH[q + 1]) - CC[n + 4] * mk(A.H[q], A.H[q + 1]);
-        }
-      const double sc = 1.0 / (1.0 + red[12][0] + CC[8].re);
       cplx ei[3], hi[3];
       force_incident(A, r, ei, hi);
       for (int l = 0; l < 3; l++) {
-        const cplx ev = es[l] * sc + ei[l], hv = hs[l] * sc + hi[l];
+        const cplx ev = es[l] + ei[l], hv = hs[l] + hi[l];
         ehs[2 * l] = ev.re; ehs[2 * l + 1] = ev.im; ehs[6 + 2 * l] = hv.re; ehs[7 + 2 * l] = hv.im;
       }
     }

@@ -257,6 +257,16 @@ int bem3_ctx_potential(bem3_ctx c, int n, const double *r, int type, int total, 
  * region), as the reference returns. */
 int bem3_ctx_field_memp(bem3_ctx c, int n, const double *r, int type, int total, double *E, double *H, int *did);
 
+/* Electromagnetic field on the boundary of the open region at n points on its elements (EH_s_bd /
+ * EH_t_bd, d3qd2_src/d3qd2_field.c:299-385): t[i] the element's 1-based position in domain did's list
+ * (the reference's t), zeta_eta [n][2] the point's parameters on it (main-domain side).  Every other
+ * element by the rule `type` (0-3), the element itself by the singular rule around the point, divided
+ * by 1 + F.  total 0: scattered field (EH_s_bd), 1: plus the incident field (EH_t_bd).  E, H: [n][3]
+ * complex.  did must be 0 and the problem quasi-periodic (BEM3_ERR_ARG otherwise: interior domains
+ * would need the free-space rule of coef_bd at arbitrary points, not provided). */
+int bem3_ctx_field_bd(bem3_ctx c, int did, int n, const int *t, const double *zeta_eta, int type, int total,
+                      double *E, double *H);
+
 /* Radiation force F[3] and torque N[3] about rc[3] on the objects, from the Maxwell stress tensor
  * of the total field on the open region's boundary (force_FN, d3qd2_src/d3qd2_force.c:10-54).
  * type 0: element nodes (plus the centroid on triangles); type 1: 9-point (quads) / 7-point

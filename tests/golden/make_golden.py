@@ -25,9 +25,11 @@ oracle/Makefile and called through oracle/reforacle.py:
                 results, from the reference's EH_t / EH_s on two planes.
   c1_sphere384.npz  plain configuration 1 end to end through the reference's own solver program
                 (see c1_fixture).
+  example2_rows.npz  the reference's EH_t (type 1) on two rows of example2.c's first plane for the
+                verification result, as the intensities that program writes.
 
 Usage: python tests/golden/make_golden.py <reference_dir> [section ...]
-       sections: gauleg faddeeva qpgf rows bv near potentials power fullsize c1 (default: all)
+       sections: gauleg faddeeva qpgf rows bv near potentials power fullsize c1 example2 (default: all)
 """
 import os
 import sys
@@ -46,7 +48,7 @@ if len(sys.argv) < 2 or not os.path.isdir(os.path.join(sys.argv[1], "d3qd2_src")
     sys.exit("usage: make_golden.py <checkout of akohta/bem3_emf_qd2> [section ...]")
 REF = sys.argv[1]
 SECTIONS = {a for a in sys.argv[2:] if "=" not in a} or {"gauleg", "faddeeva", "qpgf", "rows", "bv", "near",
-                                                         "potentials", "power", "fullsize", "c1"}
+                                                         "potentials", "power", "fullsize", "c1", "example2"}
 ONLY = {x for a in sys.argv[2:] if a.startswith("only=") for x in a[5:].split(",")}
 
 
@@ -317,10 +319,36 @@ def c1_fixture(o):
     np.savez_compressed(os.path.join(HERE, "c1_sphere384.npz"), **rec)
 
 
+EX2_ROWS = (0, 100)  # rows i of example2.c's first plane (x = 0) held by example2_rows.npz
+
+
+def example2_rows(o):
+    """The reference's EH_t, type 1, at the points of rows EX2_ROWS of the first plane that the
+    reference's example2.c evaluates (x = 0; y = -rang + i dr, z = -rang + j dr, rang = lambda_0,
+    dr = 2 rang / 199, j = 0..199; example2.c:16-45) on its verification result (veri.dat), as the
+    intensities |E|^2 and |H|^2 it writes to Ie_yz.txt / Ih_yz.txt."""
+    sub, dat = BV_CASES["veri"][0], BV_CASES["veri"][1]
+    o.load_dat(os.path.join(REF, sub, dat))
+    lam = float(o.geometry()["lambda0"])
+    rang, mx = 1.0 * lam, 200
+    dr = rang * 2.0 / (mx - 1)
+    out = {"rows": np.array(EX2_ROWS), "lambda0": np.array(lam)}
+    for i in EX2_ROWS:
+        r = np.array([[0.0, -rang + i * dr, -rang + j * dr] for j in range(mx)])
+        E, H, _ = o.EH(r, 1, total=True)
+        out[f"r{i}"] = r
+        out[f"ie{i}"] = (np.abs(E) ** 2).sum(axis=1)
+        out[f"ih{i}"] = (np.abs(H) ** 2).sum(axis=1)
+        print("example2 row", i, "done", flush=True)
+    np.savez_compressed(os.path.join(HERE, "example2_rows.npz"), **out)
+
+
 def main():
     o = RefOracle()
     if "c1" in SECTIONS:
         c1_fixture(o)
+    if "example2" in SECTIONS:
+        example2_rows(o)
     if "fullsize" in SECTIONS:
         fullsize_rows(o)
     if "power" in SECTIONS:
