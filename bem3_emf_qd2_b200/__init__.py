@@ -121,6 +121,8 @@ def lib():
         L.bem3_ctx_set_incident.argtypes = [vp, i, vp, vp, vp, vp, vp]
         L.bem3_ctx_resolve.argtypes = [vp]
         L.bem3_ctx_phase_times.argtypes = [vp, vp]
+        L.bem3_ctx_prepare.argtypes = [vp, vp]
+        L.bem3_ctx_solve_prepared.argtypes = [vp]
         L.bem3_ctx_release.argtypes = [vp]
         L.bem3_ctx_device_bytes.argtypes = [vp]
         L.bem3_ctx_device_bytes.restype = C.c_size_t
@@ -346,6 +348,18 @@ class Context:
         """method 0: reduced 4 NN system where applicable, 1: the full 8 NN system, 2: reduced only."""
         check(lib().bem3_ctx_set_solver(self.h, method), "bem3_ctx_set_solver")
         check(lib().bem3_ctx_solve(self.h), "bem3_ctx_solve")
+
+    def prepare(self) -> list:
+        """Allocates this context's matrices for an assembly outside the solve (bem3_ctx_prepare) and
+        returns every domain's bem3_batch_domain entry, to be assembled by a batch; then
+        solve_prepared() finishes the solve."""
+        arr = (bem3_batch_domain * (self.p.MN + 1))()
+        check(lib().bem3_ctx_prepare(self.h, arr), "bem3_ctx_prepare")
+        return [arr[i] for i in range(self.p.MN + 1)]
+
+    def solve_prepared(self) -> None:
+        """The solve after an external assembly of prepare()'s entries -- bem3_ctx_solve_prepared."""
+        check(lib().bem3_ctx_solve_prepared(self.h), "bem3_ctx_solve_prepared")
 
     def phase_times(self) -> dict:
         """Device time (ms) of the last solve's phases -- bem3_ctx_phase_times: the coefficient

@@ -224,12 +224,14 @@ class Tuning:
 
 
 class Batch:
-    """Every domain of `instances` (InstanceDevice) as one bem3_batch."""
+    """Every domain of `instances` (InstanceDevice) as one bem3_batch, or the given bem3_batch_domain
+    `entries` (e.g. from Context.prepare)."""
 
-    def __init__(self, instances: Sequence[InstanceDevice], tuning: Optional[Tuning] = None):
+    def __init__(self, instances: Sequence[InstanceDevice] = (), tuning: Optional[Tuning] = None, entries=None):
         from . import bem3_batch_domain, check, lib
         self.instances = list(instances)
-        entries = [e for inst in self.instances for e in inst.domain_entries()]
+        if entries is None:
+            entries = [e for inst in self.instances for e in inst.domain_entries()]
         self.n = len(entries)
         self._arr = (bem3_batch_domain * self.n)(*entries)
         self.h = C.c_void_p()
@@ -268,6 +270,20 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def assemble_entries(entries, tuning: Optional[Tuning] = None, stream=None) -> None:
+    """Assembles the matrices of the given bem3_batch_domain entries in one batch run (one graph
+    launch) and waits for it; raises if any domain fails."""
+    b = Batch(entries=list(entries), tuning=tuning)
+    try:
+        b.run(stream)
+        st = b.wait(stream)
+        bad = [x for x in st if x != 0]
+        if bad:
+            raise RuntimeError(f"batched assembly failed: status {bad[0]}")
+    finally:
+        b.close()
 
 
 # ---------------------------------------------------------------------------------------------

@@ -331,8 +331,8 @@ SolveDev solve_view_with(bem3_ctx c, SolveState& T)
   return S;
 }
 
-// Phase 1: the coefficient matrices of every domain and the node tables.
-int phase_assemble(bem3_ctx c, SolveState& T)
+// Phase 1a: the buffers of every domain's coefficient matrices and the node tables.
+int phase_alloc(bem3_ctx c, SolveState& T)
 {
   const int MN = c->MN;
   int rc;
@@ -343,11 +343,6 @@ int phase_assemble(bem3_ctx c, SolveState& T)
         T.dH[d].alloc(2 * N * N * 16) || T.dF[d].alloc(N * 3 * 8))
       return BEM3_ERR_CUDA;
     T.bytes += N * N * 16 * 6 + N * 24;
-    const int periodic = (d == 0 && c->ps == 1) ? 1 : 0;
-    rc = bem3_assemble_domain_dev(c->geo.as<double>(), c->Ne, c->dsid[d].as<int>(), ne, d, periodic, &c->qd,
-                                  c->kn[2 * d], c->kn[2 * d + 1], T.G[d].as<double>(), T.H[d].as<double>(),
-                                  T.dG[d].as<double>(), T.dH[d].as<double>(), T.dF[d].as<double>(), nullptr);
-    if (rc) return rc;
     std::vector<int> gn, cm;
     for (int t = 0; t < ne; t++) {
       const int a = abs(c->sid[d][t]);
@@ -358,6 +353,22 @@ int phase_assemble(bem3_ctx c, SolveState& T)
     }
     T.n[d] = (int)gn.size();
     if ((rc = upload(T.gnode[d], gn.data(), gn.size())) || (rc = upload(T.cmap[d], cm.data(), cm.size()))) return rc;
+  }
+  return 0;
+}
+
+// Phase 1b: the coefficient matrices of every domain (create_cmatrix, d3qd2_solve_bieq.c:156-163).
+int phase_assemble(bem3_ctx c, SolveState& T)
+{
+  int rc = phase_alloc(c, T);
+  if (rc) return rc;
+  for (int d = 0; d <= c->MN; d++) {
+    const int periodic = (d == 0 && c->ps == 1) ? 1 : 0;
+    rc = bem3_assemble_domain_dev(c->geo.as<double>(), c->Ne, c->dsid[d].as<int>(), (int)c->sid[d].size(), d,
+                                  periodic, &c->qd, c->kn[2 * d], c->kn[2 * d + 1], T.G[d].as<double>(),
+                                  T.H[d].as<double>(), T.dG[d].as<double>(), T.dH[d].as<double>(),
+                                  T.dF[d].as<double>(), nullptr);
+    if (rc) return rc;
   }
   return 0;
 }
@@ -619,6 +630,54 @@ extern "C" int bem3_ctx_solve(bem3_ctx c)
   clk.mark(3);
   c->phase_ms[0] = c->phase_ms[1] = c->phase_ms[2] = 0.0;
   clk.read(0, 3, c->phase_ms);
+  return 0;
+}
+
+extern "C" int bem3_ctx_prepare(bem3_ctx c, bem3_batch_domain* doms)
+{
+  if (!c || !doms) return BEM3_ERR_ARG;
+  DeviceGuard g(c->dev);
+  delete c->st;
+  c->st = new SolveState();
+  int rc = phase_alloc(c, *c->st);
+  if (rc) { delete c->st; c->st = nullptr; return rc; }
+  for (int d = 0; d <= c->MN; d++) {
+    bem3_batch_domain& b = doms[d];
+    SolveState& T = *c->st;
+    b.geo = c->geo.as<double>(); b.Ne = c->Ne;
+    b.sid = c->dsid[d].as<int>(); b.Ne_d = (int)c->sid[d].size(); b.did = d;
+    b.periodic = (d == 0 && c->ps == 1) ? 1 : 0;
+    b.qd = c->qd; b.kre = c->kn[2 * d]; b.kim = c->kn[2 * d + 1];
+    b.G = T.G[d].as<double>(); b.H = T.H[d].as<double>(); b.dG = T.dG[d].as<double>(); b.dH = T.dH[d].as<double>();
+    b.dF = T.dF[d].as<double>();
+  }
+  return 0;
+}
+
+extern "C" int bem3_ctx_solve_prepared(bem3_ctx c)
+{
+  if (!c || !c->st || c->st->method) return BEM3_ERR_ARG;
+  DeviceGuard g(c->dev);
+  SolveState& T = *c->st;
+  PhaseClock clk;
+  clk.mark(1);
+  SolveDev S = solve_view_with(c, T);
+  Handles& hd = thread_handles(c->dev);
+  int rc;
+  if ((rc = hd.init()) || (rc = phase_factor(c, T, S, hd))) {
+    delete c->st;
+    c->st = nullptr;
+    return rc;
+  }
+  clk.mark(2);
+  if ((rc = phase_rhs(c, T, S, hd))) {
+    delete c->st;
+    c->st = nullptr;
+    return rc;
+  }
+  clk.mark(3);
+  c->phase_ms[0] = c->phase_ms[1] = c->phase_ms[2] = 0.0;
+  clk.read(1, 3, c->phase_ms + 1);
   return 0;
 }
 

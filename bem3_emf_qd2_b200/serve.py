@@ -119,6 +119,53 @@ class GpuBackend:
         h.close()
 
 
+class BatchingGpuBackend(GpuBackend):
+    """GpuBackend whose first solves of new problems assemble together.  Workers that reach solve()
+    while an assembly is being gathered join it: the first of them waits `gather_s` for the others
+    of its admission wave, then one batch (one CUDA graph launch, bem3_batch_*) assembles every
+    domain of every problem in the wave; each worker then factorises and solves its own problem
+    (bem3_ctx_solve_prepared) concurrently with the others.  Results are those of GpuBackend: the
+    batched kernels run the same per-pair device code."""
+
+    def __init__(self, probes: Dict[str, np.ndarray], gather_s: float = 0.003):
+        super().__init__(probes)
+        self.gather_s = gather_s
+        self.cv = threading.Condition()
+        self.queue: list = []
+        self.gathering = False
+        self.waves: List[int] = []
+
+    def solve(self, h):
+        from .batch import assemble_entries
+        entries = h.prepare()
+        slot = {"done": False, "err": None}
+        with self.cv:
+            self.queue.append((entries, slot))
+            while not slot["done"]:
+                if self.gathering:
+                    self.cv.wait()
+                    continue
+                self.gathering = True
+                self.cv.wait(timeout=self.gather_s)  # the rest of the wave joins meanwhile
+                wave, self.queue = self.queue, []
+                self.cv.release()
+                err = None
+                try:
+                    assemble_entries([e for ents, _ in wave for e in ents])
+                except Exception as ex:  # every member of the wave reports it
+                    err = ex
+                finally:
+                    self.cv.acquire()
+                for _, sl in wave:
+                    sl["done"], sl["err"] = True, err
+                self.waves.append(len(wave))
+                self.gathering = False
+                self.cv.notify_all()
+        if slot["err"] is not None:
+            raise slot["err"]
+        h.solve_prepared()
+
+
 @dataclasses.dataclass
 class _Resident:
     handle: object
@@ -281,6 +328,14 @@ def run_sequential(meshes, backend, requests: List[SolveRequest]) -> List[SolveR
 
 # ---------------------------------------------------------------------------------------------
 # The served workload: a resident mesh pool and a seeded request stream
+# The served configuration's pool at the sizes one B200 can hold resident: cube-spheres 6 n^2 and
+# two-layer cube-spheres 2 x 6 n^2 from 384 elements up to 3072 (two-layer n = 16, whose resident
+# solve takes ~85 GB of the 120 GB budget by estimate_bytes; n = 18, 3888 elements, would need ~136 GB,
+# and the 12288-element two-layer meshes ~2.5 TB in this dense form).
+C5_SPHERES = (8, 10, 12, 14, 16, 18, 20)
+C5_LAYERS = (8, 9, 10, 11, 12, 13, 14, 16)
+
+
 def mesh_pool(outdir: str, sizes=(4, 5, 6, 7, 8), layers=(4, 5, 6), seed: int = 7):
     """Cube-spheres (6 n^2 quads) and two-layer cube-spheres (2 x 6 n^2) on seeded rectangular
     lattices, written in the reference's input formats and read back; returns (meshes, probes)."""
@@ -340,6 +395,52 @@ def _pct(x, q):
     return float(np.percentile(np.asarray(x), q)) if len(x) else float("nan")
 
 
+def measure(meshes, probes, requests: int = 48, workers: int = 8, budget_gb: float = 120.0, load: float = 0.8,
+            sequential: bool = True, batched: bool = True) -> dict:
+    """Served solves/s at saturation (every request queued at t = 0), p50/p99 latency under a
+    Poisson stream at `load` x that capacity, and the same requests solved one at a time by the plain
+    drop-in path (create, solve, evaluate, destroy; no reuse), on the current GPU.  batched: the
+    service's new problems assemble in batches (BatchingGpuBackend); the sequential path never does."""
+    plain = GpuBackend(probes)
+    backend = BatchingGpuBackend(probes) if batched else plain
+    budget = int(budget_gb * 1e9)
+    # warm-up: one solve per pooled mesh loads the library's kernels and the solver libraries'
+    # kernels for every system size the pool reaches (modules load lazily, on first launch)
+    for name in sorted(meshes):
+        run_sequential(meshes, plain, request_stream({name: meshes[name]}, 1, None))
+    seq = None
+    reqs0 = request_stream(meshes, requests, None)
+    if sequential:
+        t = time.perf_counter()
+        run_sequential(meshes, plain, reqs0)
+        seq = requests / (time.perf_counter() - t)
+    srv = SolveServer(meshes, backend, budget, workers)
+    t = time.perf_counter()
+    res = srv.run(reqs0)
+    cap = len(res) / (time.perf_counter() - t)
+    srv.close()
+    reqs = request_stream(meshes, requests, load * cap, seed=13)
+    srv = SolveServer(meshes, backend, budget, workers)
+    t = time.perf_counter()
+    res2 = srv.run(reqs)
+    wall = time.perf_counter() - t
+    lat = [r.latency for r in res2]
+    line = {
+        "metric": "served solves/s", "value": cap, "unit": "solves/s", "higher_is_better": True,
+        "sequential_dropin_solves_per_s": seq, "speedup_vs_sequential": (cap / seq) if seq else None,
+        "poisson": {"rate": load * cap, "solves_per_s": len(res2) / wall, "p50_s": _pct(lat, 50),
+                    "p99_s": _pct(lat, 99), "reused": sum(r.reused for r in res2), "requests": len(reqs),
+                    "completed": len(res2)},
+        "workers": workers, "hbm_budget_gb": budget_gb, "peak_reserved_gb": srv.peak_bytes / 1e9,
+        "evictions": srv.evictions, "errors": srv.errors[:3],
+        "pool": {k: int(m.Ne) for k, m in sorted(meshes.items())},
+        "batched_assembly": batched,
+        "assembly_waves": (len(backend.waves), max(backend.waves) if backend.waves else 0) if batched else None,
+    }
+    srv.close()
+    return line
+
+
 def main():
     import tempfile
     ap = argparse.ArgumentParser()
@@ -348,45 +449,16 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=120.0)
     ap.add_argument("--load", type=float, default=0.8, help="Poisson rate as a fraction of the measured capacity")
     ap.add_argument("--no-sequential", action="store_true")
+    ap.add_argument("--unbatched", action="store_true", help="each new problem assembles on its own")
+    ap.add_argument("--pool", default="small", choices=["small", "c5"],
+                    help="small: 96-432 elements; c5: 384-3072 elements (the largest resident under 120 GB)")
     args = ap.parse_args()
-    meshes, probes = mesh_pool(tempfile.mkdtemp(prefix="bem3_pool_"))
-    backend = GpuBackend(probes)
-    budget = int(args.budget_gb * 1e9)
-    # warm-up: one solve per pooled mesh loads the library's kernels and the solver libraries'
-    # kernels for every system size the pool reaches (modules load lazily, on first launch)
-    for name in sorted(meshes):
-        run_sequential(meshes, backend, request_stream({name: meshes[name]}, 1, None))
-
-    seq = None
-    reqs0 = request_stream(meshes, args.requests, None)
-    if not args.no_sequential:
-        t = time.perf_counter()
-        run_sequential(meshes, backend, reqs0)
-        seq = args.requests / (time.perf_counter() - t)
-    # capacity: every request queued at t = 0
-    srv = SolveServer(meshes, backend, budget, args.workers)
-    t = time.perf_counter()
-    res = srv.run(reqs0)
-    cap = len(res) / (time.perf_counter() - t)
-    srv.close()
-    # latency under a Poisson stream at `load` x capacity
-    reqs = request_stream(meshes, args.requests, args.load * cap, seed=13)
-    srv = SolveServer(meshes, backend, budget, args.workers)
-    t = time.perf_counter()
-    res2 = srv.run(reqs)
-    wall = time.perf_counter() - t
-    lat = [r.latency for r in res2]
-    line = {
-        "metric": "served solves/s", "value": cap, "unit": "solves/s", "higher_is_better": True,
-        "sequential_dropin_solves_per_s": seq, "speedup_vs_sequential": (cap / seq) if seq else None,
-        "poisson": {"rate": args.load * cap, "solves_per_s": len(res2) / wall, "p50_s": _pct(lat, 50),
-                    "p99_s": _pct(lat, 99), "reused": sum(r.reused for r in res2), "requests": len(reqs),
-                    "completed": len(res2)},
-        "workers": args.workers, "hbm_budget_gb": args.budget_gb, "peak_reserved_gb": srv.peak_bytes / 1e9,
-        "evictions": srv.evictions, "errors": srv.errors[:3],
-        "pool": {k: int(m.Ne) for k, m in sorted(meshes.items())},
-    }
-    srv.close()
+    if args.pool == "c5":
+        meshes, probes = mesh_pool(tempfile.mkdtemp(prefix="bem3_pool_"), C5_SPHERES, C5_LAYERS)
+    else:
+        meshes, probes = mesh_pool(tempfile.mkdtemp(prefix="bem3_pool_"))
+    line = measure(meshes, probes, args.requests, args.workers, args.budget_gb, args.load, not args.no_sequential,
+                   not args.unbatched)
     print(json.dumps(line), flush=True)
 
 

@@ -54,7 +54,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="twolayer3072")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline sampling")
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=None, help="steps of the e2e leg (default: --steps)")
+    ap.add_argument("--no-solve-stage", action="store_true", help="skip the separately timed solve stage")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-requests leg")
+    ap.add_argument("--serve-requests", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--element-stride", type=int, default=1,
                     help="keep every S-th element of each domain's list: a smaller workload with the "
@@ -222,6 +225,46 @@ def whole_job_value(pairs_per_step, steps, world, ms):
     return pairs_per_step * steps * world / (ms * 1e-3)
 
 
+def hbm_peak_gbs():
+    """The measured HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json), else the stated
+    fallback; returns (GB/s, source)."""
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = json.load(f).get("hbm_gbs")
+        if v:
+            return float(v), "MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, ValueError):
+        pass
+    return 6650.0, "fallback (earlier measurement on this pool)"
+
+
+def solve_stage(B, meshgen, configs=("sphere384", "twolayer3072")):
+    """The solve stage timed on its own (device time of bem3_ctx_solve's phases, CUDA events): the
+    coefficient matrices of every domain, the factorisations (each domain's compacted G and the
+    system of the potentials, dense LU in cuSOLVER), the right-hand sides with the boundary fields."""
+    out = {}
+    for name in configs:
+        p, _ = meshgen.problem(name, tempfile.mkdtemp(prefix="bem3_solve_"))
+        ctx = B.Context(p)
+        ctx.solve()  # first solve loads the solver libraries' kernels; timed below
+        ctx.solve()
+        ph = ctx.phase_times()
+        ctx.close()
+        out[name] = {"unknowns_reduced_system": 4 * int(p.NN), **{k: round(v, 2) for k, v in ph.items()},
+                     "solver": "reduced 4 NN system (Dirichlet-to-Neumann elimination), dense LU"}
+    return out
+
+
+def served(requests):
+    """Served solves/s and p50/p99 latency (bem3_emf_qd2_b200.serve) on its seeded pool, against the
+    same requests solved one at a time by the plain drop-in path."""
+    from bem3_emf_qd2_b200 import serve
+    pool_dir = tempfile.mkdtemp(prefix="bem3_pool_")
+    meshes, probes = serve.mesh_pool(pool_dir)
+    return serve.measure(meshes, probes, requests=requests, workers=8, budget_gb=120.0, load=0.8)
+
+
 def run_ours(args):
     import torch
     import bem3_emf_qd2_b200 as B
@@ -316,6 +359,8 @@ def run_ours(args):
 
     # end to end through the host-pointer C ABI
     e2e = None
+    if args.e2e_steps is None:
+        args.e2e_steps = args.steps
     if args.e2e_steps > 0:
         h2d = d2h = 0
         # the caller's result arrays, page-locked, allocated once (outside the timed region)
@@ -336,6 +381,28 @@ def run_ours(args):
         ems = e0.elapsed_time(e1)
         e2e = {"value": pairs * args.e2e_steps / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h}
+
+    # the matrix write-out: bytes the assembly stores per step (G, H, dG, dH, dF of every domain, the
+    # reference's layout) over the step's device time, against the HBM roofline
+    peak_hbm, hbm_src = hbm_peak_gbs()
+    wbytes = sum(16 * 6 * (4 * len(s)) ** 2 + 24 * 4 * len(s) for s in p.sid)
+    wgbs = wbytes / (ms / args.steps * 1e-3) / 1e9
+    matrix_write = {"bytes_per_step": wbytes, "gbs": wgbs, "peak_gbs": peak_hbm, "frac": wgbs / peak_hbm,
+                    "peak_source": hbm_src,
+                    "note": "average over the step; the assembly is FP64-bound, the write-out is not the limit"}
+
+    solve = None
+    if rank == 0 and not args.no_solve_stage and args.element_stride == 1:
+        try:
+            solve = solve_stage(B, meshgen)
+        except Exception as ex:  # reported, never required
+            solve = {"error": str(ex)[:300]}
+    serve_line = None
+    if rank == 0 and world == 1 and not args.no_serve and args.element_stride == 1:
+        try:
+            serve_line = served(args.serve_requests)
+        except Exception as ex:
+            serve_line = {"error": str(ex)[:300]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -359,7 +426,7 @@ def run_ours(args):
                        "parallelism": f"{world} independent instances (one per GPU)"},
             "gpu_launches": per_step_launches * args.steps,
             "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "clocks": clk,
-            "classes": classes,
+            "classes": classes, "matrix_write": matrix_write, "solve_stage": solve, "served": serve_line,
         }
         print(json.dumps(line), flush=True)
     if dist:

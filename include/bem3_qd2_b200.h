@@ -332,6 +332,15 @@ int bem3_batch_info(bem3_batch b, int *launches, size_t *device_bytes);
 
 int bem3_batch_destroy(bem3_batch b);
 
+/* A solve in two halves, so that the coefficient matrices of several contexts can be assembled
+ * together by one batch: bem3_ctx_prepare allocates the context's matrices (what bem3_ctx_solve
+ * holds) and describes every domain in doms[MN+1] (device pointers into the context; give them to
+ * bem3_batch_create, with other contexts' entries); once a batch run has filled them (after its
+ * bem3_batch_wait), bem3_ctx_solve_prepared does the rest of bem3_ctx_solve (factorisations,
+ * right-hand sides, boundary values and fields).  No counterpart in the reference (one solve_bieq per problem). */
+int bem3_ctx_prepare(bem3_ctx c, bem3_batch_domain *doms /* [MN+1] */);
+int bem3_ctx_solve_prepared(bem3_ctx c);
+
 /* Gauss-Legendre nodes and weights on [-1, 1] (the reference's gauleg, com_src/gauleg.c:3). */
 void bem3_gauss_legendre(int n, double *x, double *w);
 

@@ -221,6 +221,31 @@ void rp_assemble_rows(int did, int t0, int t1, double complex *G, double complex
   }
 }
 
+/* rp_assemble_rows with the collocation nodes of elements t0..t1 moved by `ulps` units in the last
+ * place along z (nextafter steps; the nodes are restored before return): the reference's own
+ * sensitivity to the last bit of a node's height, for rows whose sources lie in the plane of the
+ * node to within one ulp. */
+void rp_assemble_rows_zshift(int did, int t0, int t1, int ulps, double complex *G, double complex *H,
+                             double complex *dG, double complex *dH, double *dF, int nthreads)
+{
+  int t, tn, k;
+  double keep[4096][4];
+  if (t1 - t0 + 1 > 4096) return;
+  for (t = t0; t <= t1; t++) {
+    int td = abs(g_qd.bd.sb[did].sid[t]);
+    for (tn = 0; tn < 4; tn++) {
+      double *z = &(g_qd.bd.ren[td][tn][2]);
+      keep[t - t0][tn] = *z;
+      for (k = 0; k < abs(ulps); k++) *z = nextafter(*z, ulps > 0 ? INFINITY : -INFINITY);
+    }
+  }
+  rp_assemble_rows(did, t0, t1, G, H, dG, dH, dF, nthreads);
+  for (t = t0; t <= t1; t++) {
+    int td = abs(g_qd.bd.sb[did].sid[t]);
+    for (tn = 0; tn < 4; tn++) g_qd.bd.ren[td][tn][2] = keep[t - t0][tn];
+  }
+}
+
 static void set_qpd(QPD2 *q, const double *p)
 {
   q->k = p[0];

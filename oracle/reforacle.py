@@ -74,6 +74,7 @@ class RefOracle:
         lib.rp_pair.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _cp]
         lib.rp_pairs.argtypes = [C.c_int, _ip, _cp, C.c_int]
         lib.rp_assemble_rows.argtypes = [C.c_int, C.c_int, C.c_int, _cp, _cp, _cp, _cp, _dp, C.c_int]
+        lib.rp_assemble_rows_zshift.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _cp, _cp, _cp, _cp, _dp, C.c_int]
         for f in (lib.rp_qpgf_v1, lib.rp_qpgf_qG, lib.rp_qpgf_dqG):
             f.argtypes = [C.c_int, _dp, _dp, C.c_double, _cp, _ip]
         lib.rp_dcoef_rt_grad.argtypes = [C.c_int, _dp, C.c_int, C.c_int, _cp, _cp]
@@ -159,6 +160,17 @@ class RefOracle:
         dG = np.zeros((nr * 2, n), np.complex128); dH = np.zeros((nr * 2, n), np.complex128)
         dF = np.zeros((nr, 3))
         self.lib.rp_assemble_rows(did, t0, t1, G, H, dG, dH, dF, nthreads)
+        return G, H, dG, dH, dF
+
+    def assemble_rows_zshift(self, did: int, t0: int, t1: int, ulps: int, nthreads: int = 0):
+        """assemble_rows with the rows' collocation nodes moved by `ulps` units in the last place in z."""
+        ne = self.info()["Ne_d"][did]
+        n = 4 * ne
+        nr = 4 * (t1 - t0 + 1)
+        G = np.zeros((nr, n), np.complex128); H = np.zeros((nr, n), np.complex128)
+        dG = np.zeros((nr * 2, n), np.complex128); dH = np.zeros((nr * 2, n), np.complex128)
+        dF = np.zeros((nr, 3))
+        self.lib.rp_assemble_rows_zshift(did, t0, t1, ulps, G, H, dG, dH, dF, nthreads)
         return G, H, dG, dH, dF
 
     # ---- Green's function ------------------------------------------------------------

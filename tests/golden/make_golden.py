@@ -19,8 +19,10 @@ oracle/Makefile and called through oracle/reforacle.py:
   potentials.npz  the reference's mEMP_s/_t/_i (types 0-3), EH_i and EH_mEMP_s/_t/_i (types
                 0-2) at the probe points and the near-boundary points of those results.
   fullsize_rows.npz  rows of create_cmatrix_domain at the full sizes of the three plain
-                configurations (sphere384, twolayer3072, cone3360): dF, and G, H at every 8th column
-                and the element's own columns.
+                configurations (sphere384, twolayer3072, cone3360), eight elements per domain: dF,
+                and G, H (dG, dH on interior domains) at every 16th column and the element's own
+                columns; for the cone's in-plane row block also the reference's rows with the
+                collocation nodes moved by -2..2 ulps (see fullsize_rows).
   power.npz     incident, reflected and transmitted power through one unit cell for those
                 results, from the reference's EH_t / EH_s on two planes.
   c1_sphere384.npz  plain configuration 1 end to end through the reference's own solver program
@@ -209,19 +211,32 @@ def power_balance(o):
 
 
 # elements whose rows the full-size fixture holds (1-based positions in each domain's list): the
-# rows where the double-layer identity F = 1/2 is least exact, and the first element
+# rows where the double-layer identity F = 1/2 is least exact, the first element, and six more spread
+# over the list; dG, dH are kept (interior domains; the open region's are zero) for every other one
 FULLSIZE = {"sphere384": (1, 313), "twolayer3072": (1, 1536), "cone3360": (1, 69)}
-FULLSIZE_STRIDE = 8  # columns kept of each G, H row (every 8th, plus the self block)
+FULLSIZE_SPREAD = 6
+FULLSIZE_STRIDE = 16  # columns kept of each row (every 16th, plus the element's own four)
+# rows whose sources lie in the plane of the collocation nodes to within one ulp: the reference's
+# rows with those nodes moved by -2..2 ulps in z as well (its own spread there)
+FULLSIZE_ENVELOPE = {"cone3360": {0: (1,)}}
+ENVELOPE_ULPS = (-2, -1, 1, 2)
+
+
+def fullsize_elements(name, ne):
+    spread = np.unique(np.round(np.linspace(1, ne, FULLSIZE_SPREAD)).astype(int))
+    return sorted({e for e in FULLSIZE[name] if e <= ne} | set(int(e) for e in spread))
 
 
 def fullsize_rows(o):
     """Rows of create_cmatrix_domain at the three plain configurations' full sizes (meshes written
-    by bem3_emf_qd2_b200.meshgen and read by the reference's own readers): dF in full, G and H at
-    every FULLSIZE_STRIDE-th column and at the element's own four columns."""
+    by bem3_emf_qd2_b200.meshgen and read by the reference's own readers): dF in full, G and H (and
+    for every other element of the interior domains dG, dH) at every FULLSIZE_STRIDE-th column and at
+    the element's own four columns; for FULLSIZE_ENVELOPE's rows also G, H with the collocation
+    nodes moved by ENVELOPE_ULPS."""
     import tempfile
     from bem3_emf_qd2_b200 import meshgen
     out = {}
-    for name, elems in FULLSIZE.items():
+    for name in FULLSIZE:
         d = tempfile.mkdtemp(prefix="bem3_full_")
         files = meshgen.make_config(name, d)
         cwd = os.getcwd()
@@ -232,7 +247,8 @@ def fullsize_rows(o):
             os.chdir(cwd)
         info = o.info()
         for did in range(info["MN"] + 1):
-            for t in elems:
+            elems = fullsize_elements(name, info["Ne_d"][did])
+            for j, t in enumerate(elems):
                 G, H, dG, dH, dF = o.assemble_rows(did, t, t)
                 N = G.shape[1]
                 cols = np.union1d(np.arange(0, N, FULLSIZE_STRIDE), np.arange(4 * (t - 1), 4 * t))
@@ -241,6 +257,14 @@ def fullsize_rows(o):
                 out[key + "/G"] = G[:, cols]
                 out[key + "/H"] = H[:, cols]
                 out[key + "/dF"] = dF
+                if did > 0 and j % 2 == 0:
+                    out[key + "/dG"] = dG[:, cols]
+                    out[key + "/dH"] = dH[:, cols]
+                if t in FULLSIZE_ENVELOPE.get(name, {}).get(did, ()):
+                    for u in ENVELOPE_ULPS:
+                        Gs, Hs, _, _, _ = o.assemble_rows_zshift(did, t, t, u)
+                        out[f"{key}/zshift{u:+d}/G"] = Gs[:, cols]
+                        out[f"{key}/zshift{u:+d}/H"] = Hs[:, cols]
                 print(name, did, t, "done", flush=True)
     np.savez_compressed(os.path.join(HERE, "fullsize_rows.npz"), **out)
 
