@@ -29,6 +29,7 @@
 
 #include "cplx.cuh"
 #include "faddeeva.cuh"
+#include "erfcx_poly.h"
 
 #define QP_S_LIMIT 15
 #define QP_FD_LIMIT 100
@@ -37,9 +38,6 @@
 #define QP_EFS 0.1
 #define QP_MEPS 1.0e-15
 #define QP_PROP_CAP 2048  // most propagating orders a hoisted lattice list holds
-#ifndef QP_EW_REC
-#define QP_EW_REC 1  // Gaussian recurrence for the Ewald spectral rows' exponential (assembly form)
-#endif
 #ifndef QP_FD_ZFAC
 // Fourier-domain sum in the assembly's evaluation (OPT) only for |z| > QP_FD_ZFAC x split parameter:
 // (39 / 6.1) sqrt(c), c = cost of a Fourier evanescent term / cost of an Ewald one (measured on B200)
@@ -105,21 +103,34 @@ BEM_HD_NOINLINE double qp_erfc(double x) { return erfc(x); }
 #else
 BEM_HD double qp_erfc(double x) { return erfc(x); }
 #endif
-// e^{x^2} erfc(x) for x >= 0.  The host form (the host builds of these headers are test code)
-// uses the product below x = 25 and the asymptotic series above, where it converges to ~1e-18.
+// e^{x^2} erfc(x), the assembly form's Ewald spectral terms.  For x >= 0 the polynomial form of
+// erfcx_poly.h: t = P / (P + x) maps [0, inf) onto (0, 1], and erfcx(x) / t is a degree-22 polynomial
+// in s = 2 t - 1 (Chebyshev interpolant computed with mpmath by gen_erfcx_poly.py), accurate to 5e-16
+// relative on [0, 1e9).  One reciprocal and 23 multiply-adds without branches, 2.8 times cheaper than
+// CUDA's erfcx on B200 (term microbenchmark).  x < 0 (rare: a spectral term with z < 0 beyond its
+// order's Gaussian width) through erfcx(x) = 2 e^{x^2} - erfcx(-x).  Host builds evaluate the same
+// polynomial with an exact division.  QP_ERFCX_LIB selects CUDA's erfcx on the device instead.
+BEM_HD double qp_erfcx_poly(double x)  // x >= 0
+{
+  const double den = ERFCX_P + x;
+#if defined(__CUDA_ARCH__)
+  const double t = ERFCX_P * __drcp_rn(den);
+#else
+  const double t = ERFCX_P / den;
+#endif
+  const double s = 2.0 * t - 1.0;
+  double v = erfcx_c[ERFCX_DEG];
+#pragma unroll
+  for (int k = ERFCX_DEG - 1; k >= 0; k--) v = fma(v, s, erfcx_c[k]);
+  return v * t;
+}
 BEM_HD double qp_erfcx(double x)
 {
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && defined(QP_ERFCX_LIB)
   return erfcx(x);
 #else
-  if (x < 25.0) return exp(x * x) * erfc(x);
-  const double t = 1.0 / (2.0 * x * x);
-  double s = 1.0, term = 1.0;
-  for (int k = 1; k <= 10; k++) {
-    term *= -(2.0 * k - 1.0) * t;
-    s += term;
-  }
-  return s / (x * 1.7724538509055160273);
+  const double p = qp_erfcx_poly(fabs(x));
+  return (x >= 0.0) ? p : 2.0 * exp(x * x) - p;
 #endif
 }
 #if defined(QP_EXP_NOINLINE)
@@ -218,12 +229,7 @@ BEM_HD void qp_ew2_evan(const double* r, double veps, double an0, double an1, do
   if (FAST) {
     const double a = bn * veps;
     const double E = qp_exp(-(a * a + azve * azve));
-    double x1 = 0.0, x2 = 0.0;
-#pragma unroll 1
-    for (int j = 0; j < 2; j++) {
-      const double v = qp_erfcx(j == 0 ? a + azve : fabs(a - azve));
-      if (j == 0) x1 = v; else x2 = v;
-    }
+    const double x1 = qp_erfcx(a + azve), x2 = qp_erfcx_poly(fabs(a - azve));
     f1 = E * x1;
     f2 = (a >= azve) ? E * x2 : 2.0 * qp_exp(-bn * r[2]) - E * x2;
   } else {
@@ -239,27 +245,6 @@ BEM_HD void qp_ew2_evan(const double* r, double veps, double an0, double an1, do
     f2 = 1.0 / ebz * e2;
   }
   // Fn = ce / (i bn) (f1 + f2) = -i ce (f1+f2)/bn
-  F = mul_mi(ce * ((f1 + f2) * ibn));
-  dF[0] = F * an0;
-  dF[1] = F * an1;
-  dF[2] = ce * (f1 - f2);
-}
-// The FAST form with its exponential E = e^{-a^2 - b^2} = e^{(k^2 - |a_n|^2) veps^2 - z^2 / (4 veps^2)}
-// supplied by the caller, which carries it along a row of the spectral sum by a recurrence.
-BEM_HD void qp_ew2_evan_E(const double* r, double veps, double an0, double an1, double bn, double ibn, double E,
-                          cplx ce, cplx& F, cplx* dF)
-{
-  BEM_STAT_T(2);
-  const double azve = r[2] / (2.0 * veps);
-  const double a = bn * veps;
-  double x1 = 0.0, x2 = 0.0;
-#pragma unroll 1
-  for (int j = 0; j < 2; j++) {
-    const double v = qp_erfcx(j == 0 ? a + azve : fabs(a - azve));
-    if (j == 0) x1 = v; else x2 = v;
-  }
-  const double f1 = E * x1;
-  const double f2 = (a >= azve) ? E * x2 : 2.0 * qp_exp(-bn * r[2]) - E * x2;
   F = mul_mi(ce * ((f1 + f2) * ibn));
   dF[0] = F * an0;
   dF[1] = F * an1;
@@ -444,15 +429,6 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
   const int nc = L.nc1;
   const cplx E2 = expi(L.g2x * r[0] + L.g2y * r[1]);  // phase step along n2
   int dir = 0, n1 = nc, side = -1, off = 0, flg = 0;
-  // OPT Ewald rows: the factor E(n2) = e^{(k^2 - |a_n|^2) veps^2 - z^2 / (4 veps^2)} of the evanescent
-  // terms by a Gaussian recurrence along the row.  |a_n|^2 is quadratic in n2 (a_n = c + n2 g2), so
-  // E(n2 +- 1) = E(n2) R, with the ratio R itself multiplied by Cg = e^{-2 |g2|^2 veps^2} per step:
-  // two multiplications per term instead of an exponential.  Exact in exact arithmetic; each step adds
-  // about one rounding, which stays far below the terms' 1e-16 stop threshold over the row lengths here.
-  const bool rec = QP_EW_REC && OPT && !FD;
-  const double ve2 = veps * veps, azv = r[2] / (2.0 * veps);
-  const double Cg = rec ? qp_exp(-2.0 * L.g22 * ve2) : 0.0;
-  double Ec0 = 0.0, Rp0 = 0.0, Rm0 = 0.0, Ecur = 0.0, Rcur = 0.0;
   int nc2;
   if (FD) nc2 = (int)round((L.vkx * L.g2x + L.vky * L.g2y - (double)n1 * L.g12) / L.g22);
   else nc2 = (int)round(-((-L.vkx + (double)n1 * L.g1x) * L.g2x + (-L.vky + (double)n1 * L.g1y) * L.g2y) / L.g22);
@@ -467,13 +443,6 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
       const double an0 = -L.vkx + (double)n1 * L.g1x + (double)n2 * L.g2x;
       const double an1 = -L.vky + (double)n1 * L.g1y + (double)n2 * L.g2y;
       const double bn2 = L.k * L.k - an0 * an0 - an1 * an1;
-      if (rec && side < 0) {  // row centre: the recurrence's start and its first ratio on each side
-        const double adg = an0 * L.g2x + an1 * L.g2y;
-        Ec0 = qp_exp(bn2 * ve2 - azv * azv);
-        Rp0 = qp_exp(-(2.0 * adg + L.g22) * ve2);
-        Rm0 = qp_exp((2.0 * adg - L.g22) * ve2);
-        Ecur = Ec0;
-      }
       if (bn2 > 0.0) {
         e = 2;
       } else if (bn2 < 0.0) {
@@ -481,7 +450,6 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
         const double ibn = rsqrt_(-bn2);
         const double bn = -bn2 * ibn;
         if (FD) qp_fd_evan(r, an0, an1, bn, ibn, ph, F, dF);
-        else if (rec) qp_ew2_evan_E(r, veps, an0, an1, bn, ibn, Ecur, ph, F, dF);
         else qp_ew2_evan<OPT>(r, veps, an0, an1, bn, ibn, ph, F, dF);
         e = 1;
       } else {
@@ -498,7 +466,6 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
     }
     if (side < 0) {
       side = 0; off = 1; ph = ph0 * E2;
-      if (rec) { Ecur = Ec0 * Rp0; Rcur = Rp0 * Cg; }
       continue;
     }
     bool stop = false;
@@ -512,12 +479,10 @@ BEM_HD int qp_spec_sum_body(const QPLattice& L, const double* r, double veps, do
       if (off + 1 >= LIMIT) return ELIM;
       off++;
       ph = ph * (side == 0 ? E2 : conj(E2));
-      if (rec) { Ecur *= Rcur; Rcur *= Cg; }
       continue;
     }
     if (side == 0) {
       side = 1; off = 1; ph = ph0 * conj(E2);
-      if (rec) { Ecur = Ec0 * Rm0; Rcur = Rm0 * Cg; }
       continue;
     }
     // row finished

@@ -35,6 +35,7 @@ def devmath_host():
     lib = C.CDLL(so)
     vp, i, d = C.c_void_p, C.c_int, C.c_double
     lib.hm_faddeeva.argtypes = [i, vp, vp]
+    lib.hm_erfcx.argtypes = [i, vp, vp]
     lib.hm_faddeeva_fast.argtypes = [i, vp, vp]
     lib.hm_qpgf.argtypes = [i, vp, vp, i, vp, vp]
     lib.hm_qpgf2.argtypes = [i, vp, vp, vp, vp]

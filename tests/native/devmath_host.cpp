@@ -14,6 +14,12 @@ void hm_faddeeva(int n, const double* z, double* w)
   }
 }
 
+// e^{x^2} erfc(x) as the assembly's spectral terms evaluate it (qp_erfcx)
+void hm_erfcx(int n, const double* x, double* out)
+{
+  for (int i = 0; i < n; i++) out[i] = qp_erfcx(x[i]);
+}
+
 // Second derivatives: out = qG, dqG[3], d2qG[6] interleaved re/im (20 doubles per point)
 void hm_qpgf2(int n, const double* r, const double* p, double* out, int* ret)
 {

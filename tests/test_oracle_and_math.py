@@ -44,6 +44,21 @@ def test_faddeeva_host_build(devmath_host, fast):
     assert np.max(np.abs(w - f["w"]) / np.abs(f["w"])) < 1e-13
 
 
+def test_erfcx_polynomial_against_mpmath(devmath_host):
+    """The assembly's erfcx (polynomial form, csrc/erfcx_poly.h) against 50-digit mpmath over the
+    arguments the spectral terms produce (and far beyond), negative ones included: 2e-15 relative."""
+    import mpmath as mp
+    mp.mp.dps = 50
+    rng = np.random.default_rng(3)
+    x = np.concatenate([np.linspace(0.0, 8.0, 801), np.geomspace(8.0, 1e9, 200), rng.uniform(0.0, 12.0, 400),
+                        -rng.uniform(0.0, 3.0, 200)])
+    out = np.zeros_like(x)
+    devmath_host.hm_erfcx(len(x), x.ctypes.data, out.ctypes.data)
+    for xi, vi in zip(x, out):
+        ref = float(mp.exp(mp.mpf(float(xi)) ** 2) * mp.erfc(mp.mpf(float(xi))))
+        assert abs(vi - ref) <= 2e-15 * abs(ref), (xi, vi, ref)
+
+
 @pytest.mark.parametrize("mode", [0, 1])
 def test_qpgf_host_build(devmath_host, mode):
     q = golden("qpgf.npz")
