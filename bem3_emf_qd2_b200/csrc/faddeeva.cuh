@@ -99,10 +99,12 @@ BEM_HD cplx crecip_fast(cplx b)
 }
 
 // FAST selects crecip_fast for the reciprocals of the continued fraction and of the node sum.
-#if defined(FAD_W_INLINE)
-#define FAD_W_FN BEM_HD
-#else
+// Inline by default: out of line, every call from a lattice-sum loop made the loop save and restore
+// its live sums in local memory (measured 12-14 % slower on the assembly kernel).
+#if defined(FAD_W_NOINLINE)
 #define FAD_W_FN BEM_HD_NOINLINE
+#else
+#define FAD_W_FN BEM_HD
 #endif
 template <bool FAST>
 FAD_W_FN cplx faddeeva_w_upper_t(double x, double y)
@@ -112,26 +114,6 @@ FAD_W_FN cplx faddeeva_w_upper_t(double x, double y)
     BEM_STAT_W(1);
     const cplx il = crecip_fast(mk(FAD_WL + y, -x));  // 1 / (L - i z); |L - i z| >= L
     const cplx Z = mk(FAD_WL - y, x) * il;           // (L + i z) / (L - i z)
-#if defined(QP_ESTRIN)
-    // Estrin's scheme: sum_k b_k Z^k (b_k = fad_wc[N - 1 - k]) as a tree of pairs p + q Z^(2^j).
-    // About the same operations as Horner, but a dependency depth of ~6 complex steps instead of
-    // N - 1 = 39, so independent work can fill the FP64 pipe's latency.
-    static_assert(FAD_WN == 40, "the tree below is written for 40 coefficients");
-    const cplx Z2 = Z * Z, Z4 = Z2 * Z2, Z8 = Z4 * Z4, Z16 = Z8 * Z8, Z32 = Z16 * Z16;
-    cplx p1[20], p2[10], p3[5];
-#pragma unroll
-    for (int i = 0; i < 20; i++) {
-      const double b0 = fad_wc[FAD_WN - 1 - 2 * i], b1 = fad_wc[FAD_WN - 2 - 2 * i];
-      p1[i] = mk(fma(b1, Z.re, b0), b1 * Z.im);
-    }
-#pragma unroll
-    for (int i = 0; i < 10; i++) p2[i] = p1[2 * i] + p1[2 * i + 1] * Z2;
-#pragma unroll
-    for (int i = 0; i < 5; i++) p3[i] = p2[2 * i] + p2[2 * i + 1] * Z4;
-    const cplx p4a = p3[0] + p3[1] * Z8, p4b = p3[2] + p3[3] * Z8;
-    const cplx p = (p4a + p4b * Z16) + p3[4] * Z32;
-    const double pr = p.re, pi = p.im;
-#else
     double pr = fad_wc[0], pi = 0.0;
 #pragma unroll
     for (int n = 1; n < FAD_WN; n++) {
@@ -139,7 +121,6 @@ FAD_W_FN cplx faddeeva_w_upper_t(double x, double y)
       pi = pr * Z.im + pi * Z.re;
       pr = t;
     }
-#endif
     return (mk(2.0 * pr, 2.0 * pi) * il + mk(FAD_INV_SQRTPI, 0.0)) * il;
   }
   if (FAST && r2 >= 64.0 && r2 < 1.0e8) {

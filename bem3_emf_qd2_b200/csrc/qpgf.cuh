@@ -119,24 +119,9 @@ BEM_HD double qp_erfcx_poly(double x)  // x >= 0
   const double t = ERFCX_P / den;
 #endif
   const double s = 2.0 * t - 1.0;
-#if defined(QP_ESTRIN)
-  // Estrin's scheme (pairs c_2i + c_2i+1 s, then combined with s^2, s^4, s^8, s^16): dependency depth
-  // ~6 instead of 22 for about the same number of multiply-adds
-  static_assert(ERFCX_DEG == 22, "the tree below is written for degree 22");
-  const double s2 = s * s, s4 = s2 * s2, s8 = s4 * s4, s16 = s8 * s8;
-  double l1[12], l2[6];
-#pragma unroll
-  for (int i = 0; i < 11; i++) l1[i] = fma(erfcx_c[2 * i + 1], s, erfcx_c[2 * i]);
-  l1[11] = erfcx_c[22];
-#pragma unroll
-  for (int i = 0; i < 6; i++) l2[i] = fma(l1[2 * i + 1], s2, l1[2 * i]);
-  const double l3a = fma(l2[1], s4, l2[0]), l3b = fma(l2[3], s4, l2[2]), l3c = fma(l2[5], s4, l2[4]);
-  const double v = fma(l3c, s16, fma(l3b, s8, l3a));
-#else
   double v = erfcx_c[ERFCX_DEG];
 #pragma unroll
   for (int k = ERFCX_DEG - 1; k >= 0; k--) v = fma(v, s, erfcx_c[k]);
-#endif
   return v * t;
 }
 BEM_HD double qp_erfcx(double x)
