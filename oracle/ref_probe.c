@@ -221,6 +221,62 @@ void rp_assemble_rows(int did, int t0, int t1, double complex *G, double complex
   }
 }
 
+/* rp_assemble_rows for the n elements ts[] (1-based positions in domain did's list, any order),
+ * parallel over every (element, node, source) of them: rows r = 4 i + tn for element ts[i], same
+ * layout and values as rp_assemble_rows element by element.  F and its derivatives are summed per
+ * row in source order after the parallel part. */
+void rp_assemble_rows_list(int did, int n, const int *ts, double complex *G, double complex *H, double complex *dG,
+                           double complex *dH, double *dF, int nthreads)
+{
+  size_t Ne = (size_t)g_qd.bd.sb[did].Ne, N = 4 * Ne;
+  double complex kc = g_qd.kn[did];
+  long long total = (long long)n * 4 * (long long)Ne, q;
+  double *Fs = (double *)calloc((size_t)total * 3, sizeof(double));
+  if (!Fs) return;
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (q = 0; q < total; q++) {
+    int i = (int)(q / (4 * (long long)Ne)), tn = (int)((q / (long long)Ne) % 4);
+    size_t s = (size_t)(q % (long long)Ne) + 1, row = (size_t)i * 4 + tn, k;
+    int td = g_qd.bd.sb[did].sid[ts[i]], sd = g_qd.bd.sb[did].sid[s];
+    double complex CC[9], dCz[9], dCe[9];
+    double vtz[3], vte[3];
+    if (tn == 3 && ELT3 == check_element_type(td, &(g_qd.bd))) continue;
+    tz_te_bd_node(vtz, vte, td, tn, &(g_qd.bd));
+    if (did == 0 && g_qd.bd.ps == 1)
+      q0_dcoef_bd_node_t2_cc(CC, dCz, dCe, td, tn, vtz, vte, sd, kc, PREC_DEF_BE, &(g_qd.bd));
+    else
+      dcoef_bd_node_t2(CC, dCz, dCe, td, tn, vtz, vte, sd, kc, PREC_DEF_BE, &(g_qd.bd));
+    for (k = 0; k < 4; k++) {
+      G[row * N + (s - 1) * 4 + k] = CC[k];
+      H[row * N + (s - 1) * 4 + k] = CC[k + 4];
+      dG[(row * 2 + 0) * N + (s - 1) * 4 + k] = dCz[k];
+      dH[(row * 2 + 0) * N + (s - 1) * 4 + k] = dCz[k + 4];
+      dG[(row * 2 + 1) * N + (s - 1) * 4 + k] = dCe[k];
+      dH[(row * 2 + 1) * N + (s - 1) * 4 + k] = dCe[k + 4];
+    }
+    Fs[3 * q] = creal(CC[8]); Fs[3 * q + 1] = creal(dCz[8]); Fs[3 * q + 2] = creal(dCe[8]);
+  }
+  /* row sums in source order, as create_cmatrix_domain adds them (d3qd2_solve_bieq.c:222-236) */
+  for (int i = 0; i < n; i++) {
+    int td = g_qd.bd.sb[did].sid[ts[i]], tn;
+    int tl = (ELT3 == check_element_type(td, &(g_qd.bd))) ? 3 : 4;
+    for (tn = 0; tn < tl; tn++) {
+      size_t row = (size_t)i * 4 + tn, s;
+      double F = 0.0, dFz = 0.0, dFe = 0.0;
+      for (s = 0; s < Ne; s++) {
+        long long q2 = ((long long)i * 4 + tn) * (long long)Ne + (long long)s;
+        F += Fs[3 * q2]; dFz += Fs[3 * q2 + 1]; dFe += Fs[3 * q2 + 2];
+      }
+      H[row * N + (size_t)(ts[i] - 1) * 4 + tn] += (did == 0) ? 1.0 + F : F;
+      dF[row * 3 + 0] = (did == 0) ? 1.0 + F : F;
+      dF[row * 3 + 1] = dFz;
+      dF[row * 3 + 2] = dFe;
+    }
+  }
+  free(Fs);
+}
+
 /* rp_assemble_rows with the collocation nodes of elements t0..t1 moved by `ulps` units in the last
  * place along z (nextafter steps; the nodes are restored before return): the reference's own
  * sensitivity to the last bit of a node's height, for rows whose sources lie in the plane of the
@@ -239,7 +295,11 @@ void rp_assemble_rows_zshift(int did, int t0, int t1, int ulps, double complex *
       for (k = 0; k < abs(ulps); k++) *z = nextafter(*z, ulps > 0 ? INFINITY : -INFINITY);
     }
   }
-  rp_assemble_rows(did, t0, t1, G, H, dG, dH, dF, nthreads);
+  {
+    int ts[4096];
+    for (t = t0; t <= t1; t++) ts[t - t0] = t;
+    rp_assemble_rows_list(did, t1 - t0 + 1, ts, G, H, dG, dH, dF, nthreads);
+  }
   for (t = t0; t <= t1; t++) {
     int td = abs(g_qd.bd.sb[did].sid[t]);
     for (tn = 0; tn < 4; tn++) g_qd.bd.ren[td][tn][2] = keep[t - t0][tn];

@@ -74,6 +74,7 @@ class RefOracle:
         lib.rp_pair.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _cp]
         lib.rp_pairs.argtypes = [C.c_int, _ip, _cp, C.c_int]
         lib.rp_assemble_rows.argtypes = [C.c_int, C.c_int, C.c_int, _cp, _cp, _cp, _cp, _dp, C.c_int]
+        lib.rp_assemble_rows_list.argtypes = [C.c_int, C.c_int, _ip, _cp, _cp, _cp, _cp, _dp, C.c_int]
         lib.rp_assemble_rows_zshift.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _cp, _cp, _cp, _cp, _dp, C.c_int]
         for f in (lib.rp_qpgf_v1, lib.rp_qpgf_qG, lib.rp_qpgf_dqG):
             f.argtypes = [C.c_int, _dp, _dp, C.c_double, _cp, _ip]
@@ -160,6 +161,18 @@ class RefOracle:
         dG = np.zeros((nr * 2, n), np.complex128); dH = np.zeros((nr * 2, n), np.complex128)
         dF = np.zeros((nr, 3))
         self.lib.rp_assemble_rows(did, t0, t1, G, H, dG, dH, dF, nthreads)
+        return G, H, dG, dH, dF
+
+    def assemble_rows_list(self, did: int, ts, nthreads: int = 0):
+        """assemble_rows for the elements ts (1-based), parallel over every (element, node, source):
+        rows 4 i + tn for element ts[i]."""
+        ts = np.ascontiguousarray(ts, dtype=np.int32)
+        n = 4 * self.info()["Ne_d"][did]
+        nr = 4 * len(ts)
+        G = np.zeros((nr, n), np.complex128); H = np.zeros((nr, n), np.complex128)
+        dG = np.zeros((nr * 2, n), np.complex128); dH = np.zeros((nr * 2, n), np.complex128)
+        dF = np.zeros((nr, 3))
+        self.lib.rp_assemble_rows_list(did, len(ts), ts, G, H, dG, dH, dF, nthreads)
         return G, H, dG, dH, dF
 
     def assemble_rows_zshift(self, did: int, t0: int, t1: int, ulps: int, nthreads: int = 0):

@@ -248,8 +248,11 @@ def fullsize_rows(o):
         info = o.info()
         for did in range(info["MN"] + 1):
             elems = fullsize_elements(name, info["Ne_d"][did])
+            allrows = o.assemble_rows_list(did, elems)
             for j, t in enumerate(elems):
-                G, H, dG, dH, dF = o.assemble_rows(did, t, t)
+                G, H = allrows[0][4 * j:4 * j + 4], allrows[1][4 * j:4 * j + 4]
+                dG, dH = allrows[2][8 * j:8 * j + 8], allrows[3][8 * j:8 * j + 8]
+                dF = allrows[4][4 * j:4 * j + 4]
                 N = G.shape[1]
                 cols = np.union1d(np.arange(0, N, FULLSIZE_STRIDE), np.arange(4 * (t - 1), 4 * t))
                 key = f"{name}/d{did}/t{t}"
