@@ -229,6 +229,7 @@ class SolveServer:
         base = self.meshes[req.mesh]
         problem = base.with_incidence(request_waves(base, req))
         kind, what = how
+        h = None
         try:
             if kind == "reuse":
                 h = what.handle
@@ -239,6 +240,8 @@ class SolveServer:
                 self.backend.solve(h)
             E, H, did, F, N = self.backend.evaluate(h, req.mesh)
         except Exception as ex:  # keep the server alive; the request reports the failure
+            if kind == "new" and h is not None:
+                self.backend.close(h)  # a failed first solve keeps nothing on the device
             with self.lock:
                 self.errors.append(f"request {req.rid}: {ex}")
                 if kind == "new":
