@@ -202,15 +202,39 @@ __device__ __forceinline__ void reg_periodic_unit(const AssembleArgs& A, const Q
 #pragma unroll 1
   for (int j = 0; j < REGP_PAIRS; j++) {
     if (npts[j] == 0) continue;  // uniform across the warp
-    double v[19];
-    accp_pack(sacc[j][threadIdx.x], v);
-    warp_sum_arr<19>(v);
-    AccP s;
-    accp_unpack(v, s);
-    cplx CC[9], dCz[9], dCe[9];
-    accp_finish(sw[j].es, s, CC, dCz, dCe);
+    // Warp totals of the 19 sums (AccP is 19 doubles: G, H interleaved re/im, F, dF0, dF1): lane
+    // i < 19 adds component i over the warp's 32 shared-memory slots, then writes it to slot 0,
+    // which every lane reads for the one item it stores.  No per-thread arrays: the scaled
+    // coefficients never leave registers or shared memory.
+    double* acc = reinterpret_cast<double*>(&sacc[j][threadIdx.x & ~31]);
+    static_assert(sizeof(AccP) == 19 * sizeof(double), "AccP is read as 19 doubles");
+    __syncwarp();  // every lane's last accumulation is visible to the others
+    double tot = 0.0;
+    if (lane < 19) {
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+      for (int t = 0; t < 32; t += 4) {
+        s0 += acc[(t + 0) * 19 + lane];
+        s1 += acc[(t + 1) * 19 + lane];
+        s2 += acc[(t + 2) * 19 + lane];
+        s3 += acc[(t + 3) * 19 + lane];
+      }
+      tot = (s0 + s1) + (s2 + s3);
+    }
+    __syncwarp();
+    if (lane < 19) acc[lane] = tot;
+    __syncwarp();
+    // the scalings of accp_finish: quads as summed; triangles G |W| / 24, H / 24
+    double gs = 1.0, hs = 1.0, fs = EL_I_FP;
+    if (sw[j].es.nn != 4) {
+      const double V[3] = {sw[j].es.cw[0][0], sw[j].es.cw[1][0], sw[j].es.cw[2][0]};
+      gs = 1.0 / (24.0) * vnorm3(V);
+      hs = 1.0 / (24.0);
+      fs = 0.0625 * EL_SQ3 * EL_I_SPSQ3;
+    }
+    const double dFz = acc[17] * fs, dFe = acc[18] * fs;
     const long long pi = first + j;
-    if (needs_gh(dCz[8].re, dCe[8].re)) {
+    if (needs_gh(dFz, dFe)) {
       if (lane == 0) {
         unsigned slot = atomicAdd(gh_count, 1u);
         if (slot < gh_cap) gh_list[slot] = (unsigned)pi;
@@ -218,7 +242,21 @@ __device__ __forceinline__ void reg_periodic_unit(const AssembleArgs& A, const Q
       }
       continue;
     }
-    store_pair(A, q[j].row, q[j].s, CC, dCz, dCe, Fp, pi, lane);
+    // lane it stores item it of store_pair's order: G[0..3], H[0..3], the (zero) dG and dH rows, F
+    const size_t N = (size_t)4 * A.ne, col = (size_t)4 * q[j].s, row = (size_t)q[j].row;
+    const int it = lane;
+    if (it < 4) {
+      ((cplx*)A.G)[row * N + col + it] = mk(acc[2 * it] * gs, acc[2 * it + 1] * gs);
+    } else if (it < 8) {
+      ((cplx*)A.H)[row * N + col + it - 4] = mk(acc[2 * it] * hs, acc[2 * it + 1] * hs);
+    } else if (it < 16) {
+      if (A.dG) ((cplx*)A.dG)[(2 * row + (it >= 12)) * N + col + (it & 3)] = mk(0, 0);
+    } else if (it < 24) {
+      if (A.dH) ((cplx*)A.dH)[(2 * row + (it >= 20)) * N + col + (it & 3)] = mk(0, 0);
+    } else if (it == 24) {
+      Fp[pi] = make_double3(acc[16] * fs, dFz, dFe);
+    }
+    __syncwarp();  // slot 0 is rewritten by the next pair's accumulation only after every read
   }
 }
 

@@ -22,7 +22,7 @@ oracle/Makefile and called through oracle/reforacle.py:
                 configurations (sphere384, twolayer3072, cone3360), eight elements per domain: dF,
                 and G, H (dG, dH on interior domains) at every 16th column and the element's own
                 columns; for the cone's in-plane row block also the reference's rows with the
-                collocation nodes moved by -2..2 ulps (see fullsize_rows).
+                collocation nodes moved by -4..4 ulps (see fullsize_rows).
   power.npz     incident, reflected and transmitted power through one unit cell for those
                 results, from the reference's EH_t / EH_s on two planes.
   c1_sphere384.npz  plain configuration 1 end to end through the reference's own solver program
@@ -32,6 +32,7 @@ oracle/Makefile and called through oracle/reforacle.py:
 
 Usage: python tests/golden/make_golden.py <reference_dir> [section ...]
        sections: gauleg faddeeva qpgf rows bv near potentials power fullsize c1 example2 (default: all)
+                 envelope (only the z-shifted rows of an existing fullsize_rows.npz)
 """
 import os
 import sys
@@ -217,9 +218,10 @@ FULLSIZE = {"sphere384": (1, 313), "twolayer3072": (1, 1536), "cone3360": (1, 69
 FULLSIZE_SPREAD = 6
 FULLSIZE_STRIDE = 16  # columns kept of each row (every 16th, plus the element's own four)
 # rows whose sources lie in the plane of the collocation nodes to within one ulp: the reference's
-# rows with those nodes moved by -2..2 ulps in z as well (its own spread there)
+# rows with those nodes moved by -4..4 ulps in z as well (its own spread there; the range over
+# these nine rows is the same as over -8..8)
 FULLSIZE_ENVELOPE = {"cone3360": {0: (1,)}}
-ENVELOPE_ULPS = (-2, -1, 1, 2)
+ENVELOPE_ULPS = (-4, -3, -2, -1, 1, 2, 3, 4)
 
 
 def fullsize_elements(name, ne):
@@ -264,12 +266,45 @@ def fullsize_rows(o):
                     out[key + "/dG"] = dG[:, cols]
                     out[key + "/dH"] = dH[:, cols]
                 if t in FULLSIZE_ENVELOPE.get(name, {}).get(did, ()):
-                    for u in ENVELOPE_ULPS:
-                        Gs, Hs, _, _, _ = o.assemble_rows_zshift(did, t, t, u)
-                        out[f"{key}/zshift{u:+d}/G"] = Gs[:, cols]
-                        out[f"{key}/zshift{u:+d}/H"] = Hs[:, cols]
+                    out.update(envelope_rows(o, key, did, t, cols))
                 print(name, did, t, "done", flush=True)
     np.savez_compressed(os.path.join(HERE, "fullsize_rows.npz"), **out)
+
+
+def envelope_rows(o, key, did, t, cols):
+    """G, H of element t's rows with its collocation nodes moved by ENVELOPE_ULPS in z (the
+    reference loaded in `o`), at the columns `cols`."""
+    out = {}
+    for u in ENVELOPE_ULPS:
+        Gs, Hs, _, _, _ = o.assemble_rows_zshift(did, t, t, u)
+        out[f"{key}/zshift{u:+d}/G"] = Gs[:, cols]
+        out[f"{key}/zshift{u:+d}/H"] = Hs[:, cols]
+    return out
+
+
+def fullsize_envelope(o):
+    """Recomputes only the FULLSIZE_ENVELOPE rows of an existing fullsize_rows.npz (section
+    "envelope"): the other entries are kept as they are."""
+    import tempfile
+    from bem3_emf_qd2_b200 import meshgen
+    path = os.path.join(HERE, "fullsize_rows.npz")
+    g = np.load(path)
+    out = {k: g[k] for k in g.files if "/zshift" not in k}
+    for name, per in FULLSIZE_ENVELOPE.items():
+        d = tempfile.mkdtemp(prefix="bem3_env_")
+        files = meshgen.make_config(name, d)
+        cwd = os.getcwd()
+        os.chdir(d)
+        try:
+            o.load(*[os.path.basename(f) for f in files])
+        finally:
+            os.chdir(cwd)
+        for did, ts in per.items():
+            for t in ts:
+                key = f"{name}/d{did}/t{t}"
+                out.update(envelope_rows(o, key, did, t, g[key + "/cols"]))
+                print(key, "envelope done", flush=True)
+    np.savez_compressed(path, **out)
 
 
 # Plain configuration 1 end to end (sphere384): elements whose complete rows are stored (1-based
@@ -378,6 +413,8 @@ def main():
         example2_rows(o)
     if "fullsize" in SECTIONS:
         fullsize_rows(o)
+    if "envelope" in SECTIONS and "fullsize" not in SECTIONS:
+        fullsize_envelope(o)
     if "power" in SECTIONS:
         power_balance(o)
     if "near" in SECTIONS:
