@@ -182,6 +182,7 @@ class SolveServer:
         self.workers = workers
         self.lock = threading.Condition()
         self.resident: "OrderedDict[tuple, _Resident]" = OrderedDict()  # LRU order, oldest first
+        self.wanted: set = set()  # keys that queued requests ask for (kept resident when possible)
         self.reserved = 0        # estimates of problems being solved for the first time
         self.peak_bytes = 0
         self.evictions = 0
@@ -192,10 +193,13 @@ class SolveServer:
         return self.reserved + sum(r.bytes for r in self.resident.values())
 
     def _make_room(self, need: int) -> bool:
+        """Evicts idle resident problems, least recently used first among those no queued request
+        asks for, then among the rest, until `need` more bytes fit the budget."""
         while self._in_use() + need > self.budget:
             idle = [k for k, r in self.resident.items() if not r.busy]
             if not idle:
                 return False
+            idle.sort(key=lambda k: k in self.wanted)  # stable: LRU order within each group
             r = self.resident.pop(idle[0])
             self.backend.close(r.handle)
             self.evictions += 1
@@ -287,18 +291,25 @@ class SolveServer:
                     now = time.perf_counter() - t0
                     while future and future[0][0] <= now:
                         pending.append(heapq.heappop(future)[2])
-                    # admit in arrival order; a request that cannot start now does not block
-                    # later ones (continuous batching)
-                    i = 0
-                    while i < len(pending) and running < self.workers:
-                        how = self._admit(pending[i])
-                        if how is None:
-                            i += 1
-                            continue
-                        req = pending.pop(i)
-                        running += 1
-                        fut = pool.submit(self._run, req, how, t0)
-                        fut.add_done_callback(lambda f, rid=req.rid: done(f, rid))
+                    # admit requests for idle resident problems first, then the rest in arrival
+                    # order; a request that cannot start now does not block later ones
+                    # (continuous batching); problems that queued requests ask for are evicted last
+                    self.wanted = {r.key for r in pending}
+                    for reuse_pass in (True, False):
+                        i = 0
+                        while i < len(pending) and running < self.workers:
+                            r0 = self.resident.get(pending[i].key)
+                            if reuse_pass and (r0 is None or r0.busy):
+                                i += 1
+                                continue
+                            how = self._admit(pending[i])
+                            if how is None:
+                                i += 1
+                                continue
+                            req = pending.pop(i)
+                            running += 1
+                            fut = pool.submit(self._run, req, how, t0)
+                            fut.add_done_callback(lambda f, rid=req.rid: done(f, rid))
                     if not (future or pending or running):
                         break
                     wait = (future[0][0] - now) if future else 0.5

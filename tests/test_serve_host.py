@@ -127,3 +127,21 @@ def test_oversized_request_is_refused(pool):
     srv.budget = per // 10
     with pytest.raises(ValueError):
         srv.run(reqs)
+
+
+def test_queued_repeats_reuse_under_a_tight_budget(pool):
+    """All requests queued at once, room for two problems: the problems that queued requests ask
+    for are evicted last and their requests admitted first, so every polarisation repeat is served
+    from its resident factorisation although the budget forces evictions."""
+    from bem3_emf_qd2_b200 import serve
+    meshes, _ = pool
+    reqs = serve.request_stream(meshes, 30, rate=None, reuse=0.4, seed=9)
+    keys = {r.key for r in reqs}
+    assert len(reqs) - len(keys) >= 5
+    srv, be, _ = _server(pool, 2)
+    res = srv.run(reqs)
+    assert len(res) == len(reqs) and be.violations == 0
+    assert srv.peak_bytes <= srv.budget and srv.evictions > 0
+    assert be.solves == len(keys)
+    assert be.resolves == len(reqs) - len(keys)
+    srv.close()
