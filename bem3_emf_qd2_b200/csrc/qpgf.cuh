@@ -103,15 +103,19 @@ BEM_HD_NOINLINE double qp_erfc(double x) { return erfc(x); }
 #else
 BEM_HD double qp_erfc(double x) { return erfc(x); }
 #endif
-// e^{x^2} erfc(x), the assembly form's Ewald spectral terms.  For x >= 0 the polynomial form of
-// erfcx_poly.h: t = P / (P + x) maps [0, inf) onto (0, 1], and erfcx(x) / t is a degree-22 polynomial
-// in s = 2 t - 1 (Chebyshev interpolant computed with mpmath by gen_erfcx_poly.py), accurate to 5e-16
-// relative on [0, 1e9).  One reciprocal and 23 multiply-adds without branches: 434 G evaluations/s on
-// a B200 against 273 G/s for CUDA's erfcx (term microbenchmark).  x < 0 (rare: a spectral term with z < 0 beyond its
-// order's Gaussian width) through erfcx(x) = 2 e^{x^2} - erfcx(-x).  Host builds evaluate the same
-// polynomial with an exact division.  QP_ERFCX_LIB selects CUDA's erfcx on the device instead.
+// e^{x^2} erfc(x), the assembly form's Ewald spectral terms, which evaluate it at x >= 0 only (the
+// term is taken at |z|).  The polynomial form of erfcx_poly.h: t = P / (P + x) maps [0, inf) onto
+// (0, 1], and erfcx(x) / t is a degree-22 polynomial in s = 2 t - 1 (Chebyshev interpolant computed
+// with mpmath by gen_erfcx_poly.py), accurate to 5e-16 relative on [0, 1e9).  One reciprocal and 23
+// multiply-adds without branches: 434 G evaluations/s on a B200 against 273 G/s for CUDA's erfcx
+// (term microbenchmark).  Host builds evaluate the same polynomial with an exact division.
+// QP_ERFCX_LIB selects CUDA's erfcx on the device instead.  qp_erfcx extends it to x < 0 through
+// erfcx(x) = 2 e^{x^2} - erfcx(-x).
 BEM_HD double qp_erfcx_poly(double x)  // x >= 0
 {
+#if defined(__CUDA_ARCH__) && defined(QP_ERFCX_LIB)
+  return erfcx(x);
+#else
   const double den = ERFCX_P + x;
 #if defined(__CUDA_ARCH__)
   const double t = ERFCX_P * __drcp_rn(den);
@@ -123,15 +127,12 @@ BEM_HD double qp_erfcx_poly(double x)  // x >= 0
 #pragma unroll
   for (int k = ERFCX_DEG - 1; k >= 0; k--) v = fma(v, s, erfcx_c[k]);
   return v * t;
+#endif
 }
 BEM_HD double qp_erfcx(double x)
 {
-#if defined(__CUDA_ARCH__) && defined(QP_ERFCX_LIB)
-  return erfcx(x);
-#else
   const double p = qp_erfcx_poly(fabs(x));
   return (x >= 0.0) ? p : 2.0 * exp(x * x) - p;
-#endif
 }
 #if defined(QP_EXP_NOINLINE)
 BEM_HD_NOINLINE double qp_exp(double x) { return exp(x); }
@@ -227,11 +228,19 @@ BEM_HD void qp_ew2_evan(const double* r, double veps, double an0, double an1, do
   double azve = r[2] / (2.0 * veps);
   double f1, f2;
   if (FAST) {
+    // at |z| (f1 and f2 trade places under z -> -z, dF[2] changes sign below), so that both erfcx
+    // arguments but the second's in its rare branch are >= 0: no e^{x^2} branch inside erfcx
+    const double az = fabs(azve);
     const double a = bn * veps;
-    const double E = qp_exp(-(a * a + azve * azve));
-    const double x1 = qp_erfcx(a + azve), x2 = qp_erfcx_poly(fabs(a - azve));
+    const double E = qp_exp(-(a * a + az * az));
+    const double x1 = qp_erfcx_poly(a + az), x2 = qp_erfcx_poly(fabs(a - az));
     f1 = E * x1;
-    f2 = (a >= azve) ? E * x2 : 2.0 * qp_exp(-bn * r[2]) - E * x2;
+    f2 = (a >= az) ? E * x2 : 2.0 * qp_exp(-bn * fabs(r[2])) - E * x2;
+    if (r[2] < 0.0) {
+      const double t = f1;
+      f1 = f2;
+      f2 = t;
+    }
   } else {
     double ebz = qp_exp(bn * r[2]);
     // both erfc values from one call site (one copy of its code in the sums)
