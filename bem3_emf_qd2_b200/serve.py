@@ -432,6 +432,8 @@ def measure(meshes, probes, requests: int = 48, workers: int = 8, budget_gb: flo
     t = time.perf_counter()
     res = srv.run(reqs0)
     cap = len(res) / (time.perf_counter() - t)
+    cap_stats = {"reused": sum(r.reused for r in res), "evictions": srv.evictions,
+                 "peak_reserved_gb": srv.peak_bytes / 1e9}
     srv.close()
     reqs = request_stream(meshes, requests, load * cap, seed=13)
     srv = SolveServer(meshes, backend, budget, workers)
@@ -442,6 +444,7 @@ def measure(meshes, probes, requests: int = 48, workers: int = 8, budget_gb: flo
     line = {
         "metric": "served solves/s", "value": cap, "unit": "solves/s", "higher_is_better": True,
         "sequential_dropin_solves_per_s": seq, "speedup_vs_sequential": (cap / seq) if seq else None,
+        "capacity_run": cap_stats,
         "poisson": {"rate": load * cap, "solves_per_s": len(res2) / wall, "p50_s": _pct(lat, 50),
                     "p99_s": _pct(lat, 99), "reused": sum(r.reused for r in res2), "requests": len(reqs),
                     "completed": len(res2)},

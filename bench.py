@@ -40,10 +40,10 @@ ALG_OPS_PER_TERM = {"twolayer3072": 378.23, "sphere384": 377.03, "cone3360": 398
 # FP64 operations per term the hardware executed in k_reg_periodic (ncu: 2 x DFMA + DADD + DMUL,
 # thread level, over the kernel's own term counter), from the capture of the workload's /stride8
 # subsample in profiles/; None where no capture of the current kernel exists.
-HW_OPS_PER_TERM = {}
+HW_OPS_PER_TERM = {"twolayer3072": 253.6}
 # DRAM bytes (read + write) of one k_reg_periodic launch, from the same capture scaled by the
 # pairs processed (64x for stride 8).
-TRAFFIC_PER_LAUNCH = {}
+TRAFFIC_PER_LAUNCH = {"twolayer3072": 35.1e9}
 
 
 def parse():
