@@ -112,6 +112,7 @@ def lib():
                                            vp, vp, vp, vp, vp]
         L.bem3_assemble_domain_dev.argtypes = [vp, i, vp, i, i, i, C.POINTER(bem3_qpd2), d, d, vp, vp, vp, vp, vp, vp]
         L.bem3_pack_geometry.argtypes = [C.POINTER(bem3_mesh), vp]
+        L.bem3_mesh_pack_dev.argtypes = [i, i, vp, vp, vp, vp]
         L.bem3_solve_bieq_arrays.argtypes = [C.POINTER(bem3_problem), C.POINTER(bem3_bv)]
         L.bem3_ctx_create.argtypes = [C.POINTER(bem3_problem), C.POINTER(C.c_void_p)]
         L.bem3_ctx_destroy.argtypes = [vp]
@@ -195,6 +196,22 @@ class MeshArrays:
         geo = np.zeros((self.m.Ne + 1) * stride)
         check(lib().bem3_pack_geometry(C.byref(self.m), _ptr(geo)), "bem3_pack_geometry")
         return geo
+
+
+def mesh_pack_dev(rn, ed, stream=None):
+    """Geometry records of a mesh computed on the device (bem3_mesh_pack_dev): rn [Nn + 1, 3] float64
+    and ed [Ne + 1, 4] int32 torch tensors on the GPU (the reference's node table and element vertex
+    lists); returns the [(Ne + 1) * stride] float64 device tensor that bem3_pack_geometry would give."""
+    import torch
+    if rn.dtype != torch.float64 or ed.dtype != torch.int32 or not rn.is_cuda or not ed.is_cuda:
+        raise ValueError("rn must be float64 and ed int32, both on the GPU")
+    rn, ed = rn.contiguous(), ed.contiguous()
+    ne, nn = ed.shape[0] - 1, rn.shape[0] - 1
+    geo = torch.empty((ne + 1) * lib().bem3_geo_stride(), dtype=torch.float64, device=rn.device)
+    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    check(lib().bem3_mesh_pack_dev(ne, nn, C.c_void_p(rn.data_ptr()), C.c_void_p(ed.data_ptr()),
+                                   C.c_void_p(geo.data_ptr()), C.c_void_p(st)), "bem3_mesh_pack_dev")
+    return geo
 
 
 def domain_outputs(problem: Problem, did: int, derivatives: bool = True, pinned: bool = False) -> dict:

@@ -9,3 +9,4 @@
 #include "solve_dtn.cu"
 #include "context.cu"
 #include "batch.cu"
+#include "mesh.cu"

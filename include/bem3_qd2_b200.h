@@ -109,6 +109,15 @@ int bem3_assemble_domain_dev_noalloc(const double *geo_dev, int Ne, const int *s
 int bem3_geo_stride(void);
 int bem3_pack_geometry(const bem3_mesh *mesh, double *geo);
 
+/* The same geometry records computed on the device from the mesh itself: the element constants of
+ * init_elem_const (d3qd2_setup.c:1139-1186) and the collocation nodes and normals of
+ * init_boundary_data (d3qd2_setup.c:1309-1349), bit-identical to bem3_pack_geometry of the
+ * host set-up's constants.  rn_dev: [Nn + 1][3] node coordinates (row 0 unused, after any rotation
+ * and translation; read_mesh_data's dqd2.bd.rn); ed_dev: [Ne + 1][4] vertex node ids (1..Nn; the
+ * fourth 0 for a triangle; dqd2.bd.ed); geo_dev: [(Ne + 1) * bem3_geo_stride()] out.  Device
+ * pointers; synchronous on `stream`.  BEM3_ERR_ARG if an element names a node outside 1..Nn. */
+int bem3_mesh_pack_dev(int Ne, int Nn, const double *rn_dev, const int *ed_dev, double *geo_dev, void *stream);
+
 /* Counters of the last assembly on this thread: near-singular (64x64 rule) pairs. */
 unsigned long long bem3_last_gh_pairs(void);
 
