@@ -113,6 +113,8 @@ def lib():
         L.bem3_assemble_domain_dev.argtypes = [vp, i, vp, i, i, i, C.POINTER(bem3_qpd2), d, d, vp, vp, vp, vp, vp, vp]
         L.bem3_pack_geometry.argtypes = [C.POINTER(bem3_mesh), vp]
         L.bem3_mesh_pack_dev.argtypes = [i, i, vp, vp, vp, vp]
+        L.bem3_assemble_domains.argtypes = [C.POINTER(bem3_mesh), i, vp, vp, i, C.POINTER(bem3_qpd2), vp, vp, vp, vp,
+                                            vp, vp]
         L.bem3_solve_bieq_arrays.argtypes = [C.POINTER(bem3_problem), C.POINTER(bem3_bv)]
         L.bem3_ctx_create.argtypes = [C.POINTER(bem3_problem), C.POINTER(C.c_void_p)]
         L.bem3_ctx_destroy.argtypes = [vp]
@@ -255,6 +257,32 @@ def assemble_domain(problem: Problem, did: int, derivatives: bool = True, out: d
                                     _ptr(dH) if dH is not None else None, _ptr(dF))
     check(rc, "bem3_assemble_domain")
     return dict(G=G, H=H, dG=dG, dH=dH, dF=dF, gh_pairs=int(lib().bem3_last_gh_pairs()))
+
+
+def assemble_domains(problem: Problem, derivatives: bool = True, out: dict = None):
+    """Coefficient matrices of every domain in one call (bem3_assemble_domains: the reference's
+    create_cmatrix, the loop of create_cmatrix_domain over the domains), the copies of each domain's
+    matrices overlapping the later domains' kernels.  Returns {did: dict as assemble_domain};
+    `out` maps did to arrays from domain_outputs."""
+    nd = problem.MN + 1
+    outs = out if out is not None else {d: domain_outputs(problem, d, derivatives) for d in range(nd)}
+    sids = [np.ascontiguousarray(problem.sid[d], dtype=np.int32) for d in range(nd)]
+    ne = np.array([len(s) for s in sids], np.int32)
+    kn = np.array([[complex(problem.kn[d]).real, complex(problem.kn[d]).imag] for d in range(nd)], np.float64)
+    P = C.c_void_p * nd
+
+    def ptrs(key):
+        return P(*[(_ptr(outs[d][key]).value if outs[d][key] is not None else None) for d in range(nd)])
+
+    ma = MeshArrays(problem)
+    q = make_qpd(problem.qpd)
+    sid_p = P(*[_ptr(s).value for s in sids])
+    G, H, dG, dH, dF = ptrs("G"), ptrs("H"), ptrs("dG"), ptrs("dH"), ptrs("dF")
+    rc = lib().bem3_assemble_domains(C.byref(ma.m), problem.MN, sid_p, _ptr(ne), 1 if problem.ps == 1 else 0,
+                                     C.byref(q), _ptr(kn), G, H, dG, dH, dF)
+    check(rc, "bem3_assemble_domains")
+    return {d: dict(G=outs[d]["G"], H=outs[d]["H"], dG=outs[d]["dG"], dH=outs[d]["dH"], dF=outs[d]["dF"])
+            for d in range(nd)}
 
 
 class ProblemArrays:

@@ -340,6 +340,127 @@ done:
   return rc;
 }
 
+// Every domain of a problem through host pointers: the reference's create_cmatrix, the loop of
+// create_cmatrix_domain over did = 0..MN (d3qd2_solve_bieq.c:155-163).  The domains' kernels run back
+// to back on this thread's stream, the interior domains first: their matrices are large and quick to
+// compute, and the open region's long lattice sums then hide their copies.  Every finished row chunk
+// of every domain is copied on one copy stream while the later chunks compute, so only the open
+// region's last chunk is copied after the kernels end.  All domains' device matrices are held at once.
+extern "C" int bem3_assemble_domains(const bem3_mesh* mesh, int MN, const int* const* sid, const int* Ne_d, int periodic,
+                                     const bem3_qpd2* qd, const double* kn, double* const* G, double* const* H,
+                                     double* const* dG, double* const* dH, double* const* dF)
+{
+  if (!mesh || MN < 0 || !sid || !Ne_d || !kn || !G || !H) return BEM3_ERR_ARG;
+  const int Ne = mesh->Ne, nd = MN + 1;
+  for (int d = 0; d < nd; d++) {
+    if (!sid[d] || Ne_d[d] <= 0 || !G[d] || !H[d]) return BEM3_ERR_ARG;
+    for (int i = 0; i < Ne_d[d]; i++)
+      if (sid[d][i] == 0 || sid[d][i] > Ne || -sid[d][i] > Ne) return BEM3_ERR_ARG;
+  }
+  auto opt = [](double* const* a, int d) { return a ? a[d] : nullptr; };
+  std::vector<double> geo((size_t)(Ne + 1) * GEO_STRIDE);
+  int e = bem3_pack_geometry(mesh, geo.data());
+  if (e) return e;
+  std::vector<int> order;  // interior domains first, the open region (did 0) last
+  for (int d = 1; d < nd; d++) order.push_back(d);
+  order.push_back(0);
+  std::vector<size_t> N(nd);
+  std::vector<int> rows(nd);
+  size_t need = 0;
+  for (int d = 0; d < nd; d++) {
+    N[d] = (size_t)4 * Ne_d[d];
+    int r = (int)((N[d] + 7) / 8);  // about 8 row chunks per domain, as bem3_assemble_domain
+    r = r < 64 ? 64 : r;
+    r = r > default_rows_per_chunk(Ne_d[d]) ? default_rows_per_chunk(Ne_d[d]) : r;
+    rows[d] = r;
+    const size_t b = bem3_scratch_bytes(Ne_d[d], r);
+    need = b > need ? b : need;
+  }
+  double* dgeo = nullptr;
+  int* dstat = nullptr;
+  unsigned long long* dgh = nullptr;
+  std::vector<int*> dsid(nd, nullptr);
+  std::vector<double*> dG_(nd, nullptr), dH_(nd, nullptr), ddG(nd, nullptr), ddH(nd, nullptr), ddF(nd, nullptr);
+  std::vector<RowCopies> rcp(nd);
+  std::vector<DomainRun> run(nd);
+  std::vector<int> hs(nd, 0);
+  std::vector<unsigned long long> hgh(nd, 0);
+  cudaStream_t cs = nullptr;
+  const cudaStream_t st = cudaStreamPerThread;
+  int rc = BEM3_ERR_CUDA;
+  DevRes* R = nullptr;
+  // the scratch at its largest before the first launch: no domain may reallocate it under another's kernels
+  if ((rc = ensure_scratch(need, &R))) goto done;
+  rc = BEM3_ERR_CUDA;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) { cs = nullptr; goto done; }
+  if (cudaMalloc(&dgeo, geo.size() * sizeof(double)) != cudaSuccess) goto done;
+  if (cudaMalloc(&dstat, nd * sizeof(int)) != cudaSuccess) goto done;
+  if (cudaMalloc(&dgh, nd * sizeof(unsigned long long)) != cudaSuccess) goto done;
+  for (int d = 0; d < nd; d++) {
+    const size_t n2 = N[d] * N[d] * 16;
+    if (cudaMalloc(&dsid[d], Ne_d[d] * sizeof(int)) != cudaSuccess) goto done;
+    if (cudaMalloc(&dG_[d], n2) != cudaSuccess || cudaMalloc(&dH_[d], n2) != cudaSuccess) goto done;
+    if (opt(dG, d) && cudaMalloc(&ddG[d], 2 * n2) != cudaSuccess) goto done;
+    if (opt(dH, d) && cudaMalloc(&ddH[d], 2 * n2) != cudaSuccess) goto done;
+    if (opt(dF, d) && cudaMalloc(&ddF[d], 3 * N[d] * sizeof(double)) != cudaSuccess) goto done;
+    if (cudaMemcpy(dsid[d], sid[d], Ne_d[d] * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) goto done;
+    rcp[d].N = N[d];
+  }
+  if (cudaMemcpy(dgeo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) goto done;
+  for (int d : order) {
+    const ChunkHook hook = {RowCopies::hook, &rcp[d]};
+    rc = enqueue_domain(dgeo, Ne, dsid[d], Ne_d[d], d, (periodic && d == 0) ? 1 : 0, qd, kn[2 * d], kn[2 * d + 1],
+                        dG_[d], dH_[d], ddG[d], ddH[d], ddF[d], st, rows[d], &hook, run[d]);
+    if (rc) goto done;
+    rc = BEM3_ERR_CUDA;
+    if (rcp[d].failed) goto done;
+    // the domain's status word and near-singular count, kept before the next domain resets them
+    if (cudaMemcpyAsync(dstat + d, run[d].R->status, sizeof(int), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(dgh + d, run[d].S.d_gh_total, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st) !=
+            cudaSuccess)
+      goto done;
+    const size_t n = N[d];
+    for (size_t c = 0; c < rcp[d].ev.size(); c++) {
+      const size_t a = (size_t)rcp[d].r0[c], m = (size_t)rcp[d].nr[c];
+      if (cudaStreamWaitEvent(cs, rcp[d].ev[c], 0) != cudaSuccess) goto done;
+      if (cudaMemcpyAsync(G[d] + 2 * a * n, dG_[d] + 2 * a * n, m * n * 16, cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+        goto done;
+      if (cudaMemcpyAsync(H[d] + 2 * a * n, dH_[d] + 2 * a * n, m * n * 16, cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+        goto done;
+      if (ddG[d] &&
+          cudaMemcpyAsync(dG[d] + 4 * a * n, ddG[d] + 4 * a * n, 2 * m * n * 16, cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+        goto done;
+      if (ddH[d] &&
+          cudaMemcpyAsync(dH[d] + 4 * a * n, ddH[d] + 4 * a * n, 2 * m * n * 16, cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+        goto done;
+      if (ddF[d] &&
+          cudaMemcpyAsync(dF[d] + 3 * a, ddF[d] + 3 * a, 3 * m * sizeof(double), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+        goto done;
+    }
+  }
+  if (cudaStreamSynchronize(cs) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) goto done;
+  if (cudaMemcpy(hs.data(), dstat, nd * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(hgh.data(), dgh, nd * sizeof(unsigned long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+    goto done;
+  memset(&t_last_stats, 0, sizeof t_last_stats);
+  for (int d = 0; d < nd; d++) {
+    t_last_stats.gh_pairs += hgh[d];
+    t_last_stats.launches += run[d].S.launches;
+    t_last_stats.reg_periodic_launches += run[d].S.reg_periodic_launches;
+  }
+  rc = 0;
+  for (int d = 0; d < nd; d++)
+    if (hs[d]) { rc = hs[d]; break; }
+done:
+  if (cs) { cudaStreamSynchronize(cs); cudaStreamDestroy(cs); }
+  cudaDeviceSynchronize();  // nothing of this call may still use the buffers freed below
+  cudaFree(dgeo); cudaFree(dstat); cudaFree(dgh);
+  for (int d = 0; d < nd; d++) {
+    cudaFree(dsid[d]); cudaFree(dG_[d]); cudaFree(dH_[d]); cudaFree(ddG[d]); cudaFree(ddH[d]); cudaFree(ddF[d]);
+  }
+  return rc;
+}
+
 // ------------------------------------------------------------------------------------------
 // FP64 peak probe: independent DFMA chains, 8 per thread, sized so the launch runs ~100 ms.
 __global__ void __launch_bounds__(256) k_dfma_probe(double* out, int iters, double a, double b)

@@ -80,6 +80,18 @@ int bem3_assemble_domain(const bem3_mesh *mesh, const int *sid, int Ne_d, int di
                          const bem3_qpd2 *qd, double kre, double kim, double *G, double *H, double *dG,
                          double *dH, double *dF);
 
+/* Every domain of a problem in one call: the reference's create_cmatrix, the loop of
+ * create_cmatrix_domain over did = 0..MN (d3qd2_solve_bieq.c:155-163).  Domain d has sid[d]
+ * (Ne_d[d] signed ids), wave number kn[2 d] + i kn[2 d + 1] and host outputs G[d], H[d], dG[d],
+ * dH[d], dF[d] as bem3_assemble_domain's (dG, dH, dF: NULL arrays, or NULL entries, skip them);
+ * domain 0 is the quasi-periodic open region when periodic != 0.  The domains' kernels run back to
+ * back, the interior domains first, and the row chunks of every domain are copied to the host
+ * while later chunks compute; the device holds every domain's matrices at once.  Host pointers;
+ * synchronous.  Returns the first failing domain's status. */
+int bem3_assemble_domains(const bem3_mesh *mesh, int MN, const int *const *sid, const int *Ne_d, int periodic,
+                          const bem3_qpd2 *qd, const double *kn, double *const *G, double *const *H,
+                          double *const *dG, double *const *dH, double *const *dF);
+
 /* Device-resident variant.  geo_dev: packed geometry from bem3_pack_geometry (uploaded by the
  * caller); sid_dev: [Ne_d] ints; outputs in device memory.  The library allocates its scratch
  * with cudaMalloc on a calling thread's first use and keeps it, per host thread and device, for

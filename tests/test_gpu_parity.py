@@ -90,3 +90,24 @@ def test_triangle_rows_tn3_are_empty(cuda_lib):
             r = 4 * (t - 1) + 3
             assert np.abs(M["G"][r]).max() == 0 and np.abs(M["H"][r]).max() == 0 and np.abs(M["dF"][r]).max() == 0
             break
+
+
+@pytest.mark.parametrize("case", ["sphere_m4", "cone_m1", "sphere_m2"])
+def test_all_domains_call_equals_one_domain_calls(cuda_lib, case):
+    """bem3_assemble_domains (every domain in one call, copies overlapping the later domains'
+    kernels) gives each domain's matrices exactly as bem3_assemble_domain does, and the same number
+    of near-singular pairs."""
+    B = cuda_lib
+    g, p = _problem(case)
+    one, gh = {}, 0
+    for d in range(p.MN + 1):
+        one[d] = B.assemble_domain(p, d)
+        gh += one[d]["gh_pairs"]
+    allm = B.assemble_domains(p)
+    assert B.last_stats()["gh_pairs"] == gh
+    for d in range(p.MN + 1):
+        for k in ("G", "H", "dG", "dH", "dF"):
+            assert np.array_equal(allm[d][k], one[d][k]), (case, d, k)
+    part = B.assemble_domains(p, derivatives=False)  # the derivative matrices skipped
+    for d in range(p.MN + 1):
+        assert part[d]["dG"] is None and np.array_equal(part[d]["G"], one[d]["G"])
