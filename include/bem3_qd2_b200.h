@@ -87,7 +87,8 @@ int bem3_assemble_domain(const bem3_mesh *mesh, const int *sid, int Ne_d, int di
  * domain 0 is the quasi-periodic open region when periodic != 0.  The domains' kernels run back to
  * back, the interior domains first, and the row chunks of every domain are copied to the host
  * while later chunks compute; the device holds every domain's matrices at once.  Host pointers;
- * synchronous.  Returns the first failing domain's status. */
+ * synchronous.  Returns the first failing domain's status.  Fills bem3_last_gh_pairs and the
+ * gh_pairs / launches of bem3_last_stats, summed over the domains (no term counter or kernel times). */
 int bem3_assemble_domains(const bem3_mesh *mesh, int MN, const int *const *sid, const int *Ne_d, int periodic,
                           const bem3_qpd2 *qd, const double *kn, double *const *G, double *const *H,
                           double *const *dG, double *const *dH, double *const *dF);

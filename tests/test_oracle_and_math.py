@@ -184,6 +184,23 @@ def test_cabi_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_entry_points_refuse_bad_arguments_before_device_work(cuda_lib_host, tmp_path):
+    """Argument errors of the host-pointer and device set-up entry points come back as BEM3_ERR_ARG
+    before any device call (these run on a machine without a GPU)."""
+    import bem3_emf_qd2_b200 as B
+    from bem3_emf_qd2_b200 import meshgen
+    L = cuda_lib_host
+    assert L.bem3_mesh_pack_dev(0, 10, None, None, None, None) == -1
+    assert L.bem3_assemble_domains(None, 0, None, None, 0, None, None, None, None, None, None, None) == -1
+    p, _ = meshgen.problem("sphere384", str(tmp_path))
+    p.sid[1] = p.sid[1].copy()
+    p.sid[1][5] = p.Ne + 3  # an element id past the mesh
+    with pytest.raises(RuntimeError, match="invalid argument"):
+        B.assemble_domains(p, derivatives=False)
+    with pytest.raises(RuntimeError, match="invalid argument"):
+        B.assemble_domain(p, 1, derivatives=False)
+
+
 def test_cabi_library_loads():
     import bem3_emf_qd2_b200 as B
     L = B.lib()
