@@ -27,11 +27,14 @@ oracle/Makefile and called through oracle/reforacle.py:
                 results, from the reference's EH_t / EH_s on two planes.
   c1_sphere384.npz  plain configuration 1 end to end through the reference's own solver program
                 (see c1_fixture).
+  elem_const.npz  the reference's element constants and collocation nodes (cr, cw, ren, wen) for
+                the shipped meshes of rows_*.npz and the rotated result file of bv_ex2.npz.
   example2_rows.npz  the reference's EH_t (type 1) on two rows of example2.c's first plane for the
                 verification result, as the intensities that program writes.
 
 Usage: python tests/golden/make_golden.py <reference_dir> [section ...]
-       sections: gauleg faddeeva qpgf rows bv near potentials power fullsize c1 example2 (default: all)
+       sections: gauleg faddeeva qpgf rows bv near potentials power fullsize c1 example2 elemconst
+                 (default: all)
                  envelope (only the z-shifted rows of an existing fullsize_rows.npz)
 """
 import os
@@ -51,7 +54,8 @@ if len(sys.argv) < 2 or not os.path.isdir(os.path.join(sys.argv[1], "d3qd2_src")
     sys.exit("usage: make_golden.py <checkout of akohta/bem3_emf_qd2> [section ...]")
 REF = sys.argv[1]
 SECTIONS = {a for a in sys.argv[2:] if "=" not in a} or {"gauleg", "faddeeva", "qpgf", "rows", "bv", "near",
-                                                         "potentials", "power", "fullsize", "c1", "example2"}
+                                                         "potentials", "power", "fullsize", "c1", "example2",
+                                                         "elemconst"}
 ONLY = {x for a in sys.argv[2:] if a.startswith("only=") for x in a[5:].split(",")}
 
 
@@ -405,8 +409,32 @@ def example2_rows(o):
     np.savez_compressed(os.path.join(HERE, "example2_rows.npz"), **out)
 
 
+def element_constants_fixture(o):
+    """The reference's element constants and collocation nodes (init_elem_const and
+    init_boundary_data, d3qd2_setup.c:1139-1186, 1309-1349) as it holds them after reading the
+    shipped meshes (CASES) and the rotated result file of analysis_sample2 (BV_CASES["ex2"]):
+    cr, cw, ren, wen per case, beside the inputs the host set-up reads."""
+    out = {}
+    for name, (sub, msh, _) in CASES.items():
+        d = os.path.join(REF, sub)
+        files = [os.path.join(d, f) for f in ("ipw.txt", "periodicity_data.txt", "medium_data.txt", msh)]
+        o.load(*files)
+        g = o.geometry()
+        for k in ("cr", "cw", "ren", "wen"):
+            out[f"{name}/{k}"] = g[k]
+    sub, dat, msh, rot, _ = BV_CASES["ex2"]
+    d = os.path.join(REF, sub)
+    o.load_dat(os.path.join(d, dat))
+    g = o.geometry()
+    for k in ("cr", "cw", "ren", "wen"):
+        out[f"ex2/{k}"] = g[k]
+    np.savez_compressed(os.path.join(HERE, "elem_const.npz"), **out)
+
+
 def main():
     o = RefOracle()
+    if "elemconst" in SECTIONS:
+        element_constants_fixture(o)
     if "c1" in SECTIONS:
         c1_fixture(o)
     if "example2" in SECTIONS:

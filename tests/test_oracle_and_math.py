@@ -344,6 +344,30 @@ def test_ex2_fixture_matches_reference_log():
         assert abs(F[2] - log[f"F{ty}"][1]) <= 1e-10 * abs(F[2])
 
 
+@pytest.mark.parametrize("case", ["sphere_m4", "cone_m1", "sphere_m2", "ex2"])
+def test_element_setup_equals_reference(case):
+    """The host set-up's element constants and collocation nodes (dqd2.Problem) are the
+    reference's init_elem_const / init_boundary_data output bit for bit, quads, triangles and a
+    rotated mesh alike; the device set-up (bem3_mesh_pack_dev) is checked against the host set-up
+    in tests/test_gpu_mesh.py."""
+    from bem3_emf_qd2_b200.dqd2 import problem_from_arrays
+    g = golden("elem_const.npz")
+    src = golden("bv_ex2.npz" if case == "ex2" else f"rows_{case}.npz")
+    p = problem_from_arrays({k[3:]: src[k] for k in src.files if k.startswith("in/")})
+    assert np.array_equal(p.cr[1:], g[f"{case}/cr"][1:])
+    assert np.array_equal(p.cw[1:], g[f"{case}/cw"][1:])
+    nodes = [np.arange(p.nv[i]) for i in range(1, p.Ne + 1)]
+    for k, mine in (("ren", p.ren), ("wen", p.wen)):
+        ref = g[f"{case}/{k}"]
+        for i, js in enumerate(nodes, start=1):
+            if case == "ex2" and k == "ren":
+                # dat_read takes the collocation nodes from the result file (d3qd2_setup.c:419), as
+                # the build that wrote it computed them: they differ here in the last bit at most
+                assert np.all(np.abs(mine[i, js] - ref[i, js]) <= 2.3e-16 * np.maximum(np.abs(ref[i, js]), 0.125)), i
+            else:
+                assert np.array_equal(mine[i, js], ref[i, js]), (case, k, i)
+
+
 def test_rotation_reproduces_result_file_nodes():
     """Problem's rotation/translation (rotation_translation_obj) gives the node coordinates the
     reference stored in its result file, bit for bit."""
